@@ -1,0 +1,223 @@
+/*
+ * kestrel_cuda.h -- C ABI of the B200 (sm_100a) synthesis backend.
+ *
+ * This is the drop-in boundary for Kestrel's `Backend` trait
+ * (src/backend.rs:22-58). Every entry point below replaces one trait method
+ * (cited per function), takes plain pointers and sizes, copies what it keeps
+ * before returning, and reports failure as a non-zero status with a message
+ * readable through kc_last_error(). A context is single-threaded, exactly like
+ * the trait object it replaces (one driver thread, strictly sequential calls);
+ * it owns one CUDA stream.
+ *
+ * Byte layouts of kc_spawn_cmd and kc_region_params match the reference's
+ * repr(C) structs field for field, so the Rust side can pass its slices
+ * straight through (bytemuck::cast_slice).
+ */
+#ifndef KESTREL_CUDA_H
+#define KESTREL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define KC_OK 0
+#define KC_ERR_INVALID 1   /* bad argument: size, index, layout */
+#define KC_ERR_CUDA 2      /* a CUDA call failed */
+#define KC_ERR_OOM 3       /* device or pinned memory exhausted */
+#define KC_ERR_DEVICE 4    /* a kernel reported an internal error word */
+
+/* ---- layouts shared with the reference ---------------------------------- */
+
+/* Envelope stages, src/voice.rs:11-15. Part of the host/device contract. */
+#define KC_ENV_ATTACK 0u
+#define KC_ENV_DECAY 1u
+#define KC_ENV_SUSTAIN 2u
+#define KC_ENV_RELEASE 3u
+#define KC_ENV_DEAD 4u
+
+/* Gate table width: 16 channels x 128 keys, src/voice.rs:18. */
+#define KC_GATE_SLOTS 2048u
+/* Channel controller rows, src/voice.rs:454-463. */
+#define KC_BEND_CHANNELS 16u
+#define KC_CHAN_FIELDS 4u
+#define KC_CHAN_BEND 0u
+#define KC_CHAN_GAIN_L 1u
+#define KC_CHAN_GAIN_R 2u
+#define KC_CHAN_VARIANT 3u
+
+/* Voice flags, src/bank.rs:13-15; region-params flag, src/bank.rs:190. */
+#define KC_VF_LOOP 1u
+#define KC_VF_LOOP_UNTIL_RELEASE 2u
+#define KC_RP_FILTER 1u
+
+/* One voice's birth record. Mirrors voice::SpawnCmd (src/voice.rs:22-57):
+ * 19 x 32-bit words, 76 bytes, tightly packed. */
+typedef struct kc_spawn_cmd {
+    uint32_t phase_lo;
+    uint32_t phase_hi;
+    uint32_t step_lo;
+    uint32_t step_hi;
+    uint32_t smp_base;
+    uint32_t smp_len;
+    uint32_t loop_start;
+    uint32_t loop_end;
+    uint32_t flags;
+    uint32_t params;
+    uint32_t variant;
+    uint32_t region;
+    uint32_t gate_slot;
+    uint32_t ordinal;
+    uint32_t start_rel;
+    uint32_t note_id_lo;
+    uint32_t note_id_hi;
+    float gain_l;
+    float gain_r;
+} kc_spawn_cmd;
+
+/* Per-(region, key, velocity) DSP constants. Mirrors bank::RegionParams
+ * (src/bank.rs:166-188): 12 x 32-bit words, 48 bytes. */
+typedef struct kc_region_params {
+    float attack_rate;
+    float attack_end;
+    float decay_coef;
+    float decay_target;
+    float sustain;
+    float release_coef;
+    float b0;
+    float b1;
+    float a1;
+    float a2;
+    uint32_t flags;
+    uint32_t pad;
+} kc_region_params;
+
+/* Mirrors backend::BlockStats (src/backend.rs:11-20). */
+typedef struct kc_block_stats {
+    uint64_t active_voices; /* live voices after the last compaction */
+    uint64_t stolen;        /* cumulative */
+    uint64_t dropped;       /* cumulative */
+    float peak;             /* max |sample| of the last block */
+    uint32_t pad;
+} kc_block_stats;
+
+/* Rules, src/config.rs:11-109 (the enum discriminants are the reference's). */
+#define KC_INTERP_NEAREST 0u
+#define KC_INTERP_LINEAR 1u
+#define KC_INTERP_CUBIC 2u
+#define KC_CURVE_EXPONENTIAL 0u
+#define KC_CURVE_LINEAR 1u
+#define KC_STEAL_OLDEST 0u
+#define KC_STEAL_DROP_NEW 1u
+#define KC_STEAL_QUIETEST 2u
+#define KC_ADMIT_LOUDEST 0u
+#define KC_ADMIT_EVEN 1u
+
+/* Mixdown arithmetic of the stereo block. */
+#define KC_MIX_F32_TREE 0u     /* fixed-order f32 tree (the reference's device form) */
+#define KC_MIX_TWO_SUM 1u      /* fixed-order tree with compensated two-sum carries */
+
+/* The subset of config::Config (src/config.rs:164-343) that the backend reads,
+ * plus the backend's own tunables. Fill with kc_config_default() first. */
+typedef struct kc_config {
+    uint32_t sample_rate;        /* Hz, 48000 */
+    uint32_t block_frames;       /* frames per render, 4096; a multiple of 16 */
+    uint32_t gate_frames;        /* gate/controller tile, 32; a multiple of 16 or a divisor of 16 */
+    uint32_t max_voices;         /* pool ceiling surviving a block */
+    uint32_t max_steal_percent;  /* 1..=100, 25 */
+    uint32_t steal_fade_frames;  /* 1..block_frames, 96 */
+    uint32_t steal_rule;         /* KC_STEAL_*, Quietest */
+    uint32_t admit_rule;         /* KC_ADMIT_*, Loudest */
+    uint32_t interpolation;      /* KC_INTERP_*, Linear */
+    uint32_t decay_curve;        /* KC_CURVE_*, Exponential */
+    uint32_t release_curve;      /* KC_CURVE_*, Exponential */
+    float env_floor;             /* 1e-5 */
+    uint32_t sort_voices;        /* 1: re-sort the pool by (region, stage, phase) */
+    uint32_t max_param_variants; /* params-table copies, 32 */
+    uint32_t mix_mode;           /* KC_MIX_*, F32 tree */
+    uint32_t strict_fp;          /* 1: no FMA contraction anywhere in the voice DSP */
+    uint32_t device;             /* CUDA ordinal */
+    uint32_t reserved[7];
+} kc_config;
+
+typedef struct kc_synth kc_synth;
+
+/* Defaults of config.rs:345-409 for every field above. */
+int kc_config_default(kc_config* cfg);
+
+/* The pool size the backend allocates for a config: max_voices plus the
+ * steal headroom, config.rs:542-552. */
+uint32_t kc_pool_slots(const kc_config* cfg);
+
+/* Replaces GpuSynth::new (src/gpu/mod.rs:276). Copies the i16 sample pool and
+ * the variant-0 params table to the device. `n_regions` and `max_sample_len`
+ * size the pool sort key exactly as SortKeyLayout::plan does
+ * (src/gpu/mod.rs:77-105). */
+int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len,
+                    const kc_region_params* params, uint32_t params_len,
+                    uint32_t n_regions, uint32_t max_sample_len, kc_synth** out);
+void kc_synth_destroy(kc_synth* s);
+
+/* Backend::set_gates (src/backend.rs:23-25): tiles * KC_GATE_SLOTS words,
+ * tile-major; tiles = block_frames / gate_frames. */
+int kc_set_gates(kc_synth* s, const uint32_t* rows, size_t n);
+
+/* Backend::set_channels (src/backend.rs:27-33): tiles * 16 * 4 words. */
+int kc_set_channels(kc_synth* s, const uint32_t* rows, size_t n, int bend, int gain,
+                    int variant);
+
+/* Backend::set_params_variant (src/backend.rs:35-39). Index 0 is the bank's
+ * own table and is left untouched, as CpuSynth does (src/cpu.rs:313-323). */
+int kc_set_params_variant(kc_synth* s, uint32_t index, const kc_region_params* data,
+                          size_t n);
+
+/* Backend::spawn (src/backend.rs:41-43). The commands are validated and
+ * copied; steal/drop/admit happen on the device inside the next render. */
+int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n);
+
+/* Backend::render (src/backend.rs:45-47): `out` receives block_frames * 2
+ * interleaved stereo floats. Blocks until the block is on the host. */
+int kc_render(kc_synth* s, float* out, size_t n);
+
+/* Backend::stats (src/backend.rs:49). */
+int kc_stats(kc_synth* s, kc_block_stats* out);
+
+/* Backend::name (src/backend.rs:51). */
+const char* kc_name(const kc_synth* s);
+
+/* Backend::timings (src/backend.rs:53-57): per-pass device milliseconds of
+ * the last render when timing is enabled (kc_set_profile). */
+int kc_set_profile(kc_synth* s, int on);
+int kc_timings(kc_synth* s, const char** names, double* ms, size_t cap, size_t* n);
+
+/* Message of the last failing call on this thread ("" when none). */
+const char* kc_last_error(void);
+
+/* ---- device-resident form ---------------------------------------------- *
+ * The same block with its inputs already in device memory: no host copies
+ * and no synchronisation. A streaming caller (or the benchmark) stages the
+ * inputs of many blocks in HBM and enqueues blocks back to back. Pointers
+ * must stay valid until the block has executed (kc_synchronize). */
+int kc_enqueue_block_device(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan,
+                            int bend, int gain, int variant, const kc_spawn_cmd* d_cmds,
+                            uint32_t n_cmds, float* d_out);
+int kc_synchronize(kc_synth* s);
+/* The context's cudaStream_t, for event timing by the caller. */
+void* kc_stream(kc_synth* s);
+/* Number of kernel launches one block enqueues (the captured graph's nodes). */
+int kc_block_launches(kc_synth* s, uint32_t* out);
+
+/* ---- inspection (tests) ------------------------------------------------- *
+ * Copies the live part of the voice pool to the host as 24 SoA fields of
+ * `*live` words each (field-major, stride `*live`), in the field order of
+ * shaders/common.wgsl:15-43. `cap_words` bounds `fields`. */
+int kc_read_pool(kc_synth* s, uint32_t* fields, size_t cap_words, uint32_t* live);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KESTREL_CUDA_H */

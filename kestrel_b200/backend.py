@@ -1,0 +1,130 @@
+"""CudaSynth: the Backend trait (src/backend.rs:22-58) over the CUDA library.
+
+Method names, argument meaning and error behaviour mirror the reference trait
+so a test reads like the reference's own: ``set_gates``, ``set_channels``,
+``set_params_variant``, ``spawn``, ``render``, ``stats``, ``name``,
+``timings``. Failures raise ``KestrelError`` carrying the library's message
+(the reference returns ``anyhow::Result``).
+
+This class only marshals arguments; every pass of the block runs in
+libkestrel_cuda.so on the GPU. Constructing it without the built library, or
+without a CUDA device, raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native as N
+
+
+@dataclass
+class BlockStats:
+    """backend::BlockStats (src/backend.rs:11-20)."""
+    active_voices: int
+    stolen: int
+    dropped: int
+    peak: float
+
+
+class CudaSynth:
+    def __init__(self, cfg: N.KcConfig, pool: np.ndarray, params: np.ndarray, n_regions: int,
+                 max_sample_len: int):
+        self._lib = N.cuda_lib()
+        self.cfg = cfg
+        pool = np.ascontiguousarray(pool, dtype=np.int16)
+        params = np.ascontiguousarray(params, dtype=N.PARAMS_DTYPE)
+        h = C.c_void_p()
+        N.check(self._lib.kc_synth_create(C.byref(cfg), N.ptr(pool) if pool.size else None, pool.size,
+                                          N.ptr(params), params.size, n_regions, max_sample_len,
+                                          C.byref(h)), self._lib)
+        self._h = h
+        self.block_frames = cfg.block_frames
+        self.tiles = cfg.block_frames // cfg.gate_frames
+        self.params_per = params.size
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.kc_synth_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- Backend trait -------------------------------------------------------
+    def set_gates(self, rows: np.ndarray) -> None:
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        N.check(self._lib.kc_set_gates(self._h, N.ptr(rows), rows.size), self._lib)
+
+    def set_channels(self, rows: np.ndarray, bend: bool, gain: bool, variant: bool) -> None:
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        N.check(self._lib.kc_set_channels(self._h, N.ptr(rows), rows.size, int(bend), int(gain),
+                                          int(variant)), self._lib)
+
+    def set_params_variant(self, index: int, data: np.ndarray) -> None:
+        data = np.ascontiguousarray(data, dtype=N.PARAMS_DTYPE)
+        N.check(self._lib.kc_set_params_variant(self._h, index, N.ptr(data), data.size), self._lib)
+
+    def spawn(self, cmds: np.ndarray) -> None:
+        cmds = np.ascontiguousarray(cmds, dtype=N.SPAWN_DTYPE)
+        N.check(self._lib.kc_spawn(self._h, N.ptr(cmds) if cmds.size else None, cmds.size), self._lib)
+
+    def render(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.block_frames * 2, dtype=np.float32)
+        N.check(self._lib.kc_render(self._h, N.ptr(out), out.size), self._lib)
+        return out
+
+    def stats(self) -> BlockStats:
+        s = N.KcBlockStats()
+        N.check(self._lib.kc_stats(self._h, C.byref(s)), self._lib)
+        return BlockStats(s.active_voices, s.stolen, s.dropped, s.peak)
+
+    def name(self) -> str:
+        return self._lib.kc_name(self._h).decode()
+
+    def set_profile(self, on: bool) -> None:
+        N.check(self._lib.kc_set_profile(self._h, int(on)), self._lib)
+
+    def timings(self) -> list[tuple[str, float]]:
+        names = (C.c_char_p * 8)()
+        ms = (C.c_double * 8)()
+        n = C.c_size_t()
+        N.check(self._lib.kc_timings(self._h, names, ms, 8, C.byref(n)), self._lib)
+        return [(names[i].decode(), ms[i]) for i in range(n.value)]
+
+    # ---- device-resident form and inspection --------------------------------
+    def enqueue_block_device(self, d_gates: int, d_chan: int, bend: bool, gain: bool, variant: bool,
+                             d_cmds: int, n_cmds: int, d_out: int) -> None:
+        N.check(self._lib.kc_enqueue_block_device(self._h, d_gates, d_chan, int(bend), int(gain),
+                                                  int(variant), d_cmds or None, n_cmds, d_out),
+                self._lib)
+
+    def synchronize(self) -> None:
+        N.check(self._lib.kc_synchronize(self._h), self._lib)
+
+    def stream(self) -> int:
+        return self._lib.kc_stream(self._h)
+
+    def block_launches(self) -> int:
+        n = C.c_uint32()
+        N.check(self._lib.kc_block_launches(self._h, C.byref(n)), self._lib)
+        return n.value
+
+    def read_pool(self) -> np.ndarray:
+        """The live voice pool as a (24, live) u32 array, field-major."""
+        st = self.stats()
+        cap = max(int(st.active_voices), 1) * 24 + 24 * 1024
+        buf = np.empty(cap, dtype=np.uint32)
+        live = C.c_uint32()
+        N.check(self._lib.kc_read_pool(self._h, N.ptr(buf), buf.size, C.byref(live)), self._lib)
+        n = live.value
+        return buf[: 24 * n].reshape(24, n).copy()

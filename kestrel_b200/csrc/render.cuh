@@ -1,0 +1,443 @@
+// render.cuh -- the per-voice render pass and the mixdown reduction.
+//
+// One lane owns one voice for the whole block, its state in registers, exactly
+// the reference's execution model (shaders/render.wgsl:146-421): the
+// sequential parts of the DSP (32.32 phase accumulator, envelope, biquad
+// memory) never round-trip through memory. What differs is how the block mix
+// is formed on sm_100a:
+//
+//   * every 16 frames a warp writes its 32 voices x 32 output slots
+//     (16 frames x 2 channels) into its own padded shared-memory tile and
+//     transpose-reduces it: lane l sums row l with four-wide loads, so each
+//     lane ends with one output slot. No block-wide barrier is ever taken.
+//   * each warp owns a 32 KiB slice of the partial buffer (L2-resident); its
+//     later voice batches accumulate into it in batch order.
+//   * a second kernel folds the warps' slices in a fixed order.
+//
+// No float atomics anywhere, and every summation order is a function of the
+// live count and the grid alone, so reruns are byte-identical.
+//
+// Bit-exactness: the envelope, the steal-key inputs and the 32.32 phase are
+// computed with explicitly rounded intrinsics (__fadd_rn/__fmul_rn), which can
+// never be contracted into an FMA, statement for statement as src/cpu.rs:
+// 403-613 orders them. With STRICT the interpolation, biquad, fade and stereo
+// gain are written the same way, so each voice's per-frame contribution is
+// bit-identical to the CPU restatement's f32 value and only the summation
+// order of the mix differs.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace kc {
+
+struct RenderArgs {
+    uint32_t* pool;            // current pool, field-major
+    uint32_t cap;              // field stride in words
+    const int16_t* pcm;        // sample pool
+    uint32_t pcm_len;          // i16 frames in it
+    const kc_region_params* params;  // n_slots copies of params_per
+    uint32_t params_per;
+    uint32_t n_slots;
+    const uint32_t* gates;     // tiles x 2048
+    const uint32_t* chan;      // tiles x 64
+    const BlockCtl* ctl;
+    DevState* st;
+    float* partial;            // [warps][2 * block_frames]
+    float* partial_c;          // two-sum carries, same shape (MIX two-sum only)
+    uint32_t block_frames;
+    uint32_t gate_frames;
+    uint32_t fade;             // steal_fade_frames
+    float env_floor;
+    uint32_t exp_decay;
+    uint32_t exp_release;
+};
+
+// Sample fetch, CpuSynth::fetch (src/cpu.rs:187-194): i16 / 32767 clamped at
+// -1, out-of-range reads as zero.
+__device__ __forceinline__ float fetch_sample(const int16_t* __restrict__ pcm, uint32_t pcm_len,
+                                              uint32_t base, uint32_t idx) {
+    const uint32_t i = base + idx;
+    const int16_t v = i < pcm_len ? __ldg(pcm + i) : (int16_t)0;
+    return fmaxf(__fmul_rn((float)v, 1.0f / 32767.0f), -1.0f);
+}
+
+// CpuSynth::advance_index (src/cpu.rs:242-259), general form in i64.
+__device__ __forceinline__ uint32_t neighbour(uint32_t idx, int off, bool looping, uint32_t ls,
+                                             uint32_t le, uint32_t len) {
+    const int64_t raw = (int64_t)idx + off;
+    if (looping) {
+        if (raw >= (int64_t)le) {
+            int64_t span = (int64_t)le - (int64_t)ls;
+            if (span < 1) span = 1;
+            return (uint32_t)((int64_t)ls + (raw - (int64_t)ls) % span);
+        }
+        if (raw < 0) return 0;
+        return (uint32_t)raw;
+    }
+    int64_t hi = (int64_t)len - 1;
+    int64_t r = raw < 0 ? 0 : raw;
+    return (uint32_t)(r > hi ? hi : r);
+}
+
+template <bool STRICT>
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
+struct VoiceRegs {
+    uint64_t phase, step, base_step;
+    uint32_t base, len, ls, le;
+    uint32_t stage;
+    float level;
+    float gl, gr, bgl, bgr;
+    float z1, z2;
+    // region params in force
+    float ar, ae, dc, dt, sus, rc, b0, b1, a1, a2;
+    bool filt;
+    bool loop_en, lur;
+    uint32_t params_base, variant, born, born_gate;
+    uint32_t slot, ordinal, start_rel, stop_rel, channel;
+};
+
+__device__ __forceinline__ void load_params(VoiceRegs& v, const RenderArgs& a, uint32_t variant) {
+    const uint32_t s = variant < a.n_slots ? variant : 0u;
+    const float4* p = reinterpret_cast<const float4*>(a.params + (size_t)s * a.params_per + v.params_base);
+    const float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
+    v.ar = q0.x; v.ae = q0.y; v.dc = q0.z; v.dt = q0.w;
+    v.sus = q1.x; v.rc = q1.y; v.b0 = q1.z; v.b1 = q1.w;
+    v.a1 = q2.x; v.a2 = q2.y;
+    v.filt = (__float_as_uint(q2.z) & KC_RP_FILTER) != 0u;
+}
+
+// Per-frame voice step. Returns the filtered, faded sample y (before the
+// stereo gains). Mirrors src/cpu.rs:490-601 for one frame; the caller has
+// already applied the f < start_rel and DEAD gates.
+template <int INTERP, bool STRICT>
+__device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, uint32_t f,
+                                             bool looping) {
+    const uint32_t idx = (uint32_t)(v.phase >> 32);
+    if (!looping && idx >= v.len) {
+        v.stage = ENV_DEAD;
+        return 0.0f;
+    }
+    // Envelope before the sample (src/cpu.rs:508-549).
+    if (v.stage == ENV_ATTACK) {
+        v.level = __fadd_rn(v.level, v.ar);
+        if (v.level >= v.ae) {
+            v.stage = ENV_DECAY;
+            v.level = 1.0f;
+        }
+    } else if (v.stage == ENV_DECAY) {
+        v.level = a.exp_decay ? __fmul_rn(v.level, v.dc) : __fsub_rn(v.level, v.dc);
+        if (v.level <= v.dt) {
+            if (v.sus <= a.env_floor) {
+                v.stage = ENV_DEAD;
+                v.level = 0.0f;
+            } else {
+                v.stage = ENV_SUSTAIN;
+                v.level = v.sus;
+            }
+        }
+    } else if (v.stage == ENV_RELEASE) {
+        v.level = a.exp_release ? __fmul_rn(v.level, v.rc) : __fsub_rn(v.level, v.rc);
+        if (v.level <= a.env_floor) {
+            v.stage = ENV_DEAD;
+            v.level = 0.0f;
+        }
+    }
+
+    // Interpolation (src/cpu.rs:261-302).
+    float s;
+    const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
+    if (INTERP == KC_INTERP_NEAREST) {
+        s = fetch_sample(a.pcm, a.pcm_len, v.base, idx);
+    } else if (INTERP == KC_INTERP_LINEAR) {
+        uint32_t i1;
+        if (looping) {
+            i1 = idx + 1u < v.le && idx != 0xFFFFFFFFu ? idx + 1u
+                                                       : neighbour(idx, 1, true, v.ls, v.le, v.len);
+        } else {
+            i1 = idx + 1u < v.len ? idx + 1u : v.len - 1u;
+        }
+        const float s0 = fetch_sample(a.pcm, a.pcm_len, v.base, idx);
+        const float s1 = fetch_sample(a.pcm, a.pcm_len, v.base, i1);
+        if (STRICT) {
+            s = __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac));
+        } else {
+            s = fmaf(s1 - s0, frac, s0);
+        }
+    } else {
+        const uint32_t im1 = neighbour(idx, -1, looping, v.ls, v.le, v.len);
+        const uint32_t i1 = neighbour(idx, 1, looping, v.ls, v.le, v.len);
+        const uint32_t i2 = neighbour(idx, 2, looping, v.ls, v.le, v.len);
+        const float sm1 = fetch_sample(a.pcm, a.pcm_len, v.base, im1);
+        const float s0 = fetch_sample(a.pcm, a.pcm_len, v.base, idx);
+        const float s1 = fetch_sample(a.pcm, a.pcm_len, v.base, i1);
+        const float s2 = fetch_sample(a.pcm, a.pcm_len, v.base, i2);
+        // catmull_rom, src/cpu.rs:297-302, left to right, always rounded per op.
+        const float ca = __fadd_rn(__fsub_rn(__fadd_rn(__fmul_rn(-0.5f, sm1), __fmul_rn(1.5f, s0)),
+                                             __fmul_rn(1.5f, s1)),
+                                   __fmul_rn(0.5f, s2));
+        const float cb = __fsub_rn(__fadd_rn(__fsub_rn(sm1, __fmul_rn(2.5f, s0)), __fmul_rn(2.0f, s1)),
+                                   __fmul_rn(0.5f, s2));
+        const float cc = __fadd_rn(__fmul_rn(-0.5f, sm1), __fmul_rn(0.5f, s1));
+        s = __fadd_rn(__fmul_rn(__fadd_rn(__fmul_rn(__fadd_rn(__fmul_rn(ca, frac), cb), frac), cc), frac), s0);
+    }
+
+    const float g = fminf(v.level, 1.0f);
+    const float x = __fmul_rn(s, g);
+    float y = x;
+    if (v.filt) {
+        // Transposed direct form II, b2 == b0 (src/cpu.rs:564-572).
+        if (STRICT) {
+            const float bx = __fmul_rn(v.b0, x);
+            y = __fadd_rn(bx, v.z1);
+            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
+            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
+        } else {
+            y = fmaf(v.b0, x, v.z1);
+            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
+            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
+        }
+    }
+    // Steal fade after the filter (src/cpu.rs:574-587).
+    if (v.stop_rel != 0u && f + 1u >= v.stop_rel) {
+        const uint32_t d = f + 1u - v.stop_rel;
+        if (d >= a.fade) {
+            v.stage = ENV_DEAD;
+            y = 0.0f;
+        } else {
+            y = __fmul_rn(y, __fsub_rn(1.0f, __fdiv_rn((float)d, (float)a.fade)));
+        }
+    }
+    // Phase advance and loop wrap (src/cpu.rs:592-601).
+    v.phase += v.step;
+    if (looping) {
+        uint32_t hi = (uint32_t)(v.phase >> 32);
+        if (hi >= v.le) {
+            uint32_t span = v.le - v.ls;
+            if (span < 1u) span = 1u;
+            hi = v.ls + (hi - v.ls) % span;
+            v.phase = ((uint64_t)hi << 32) | (uint32_t)v.phase;
+        }
+    }
+    return y;
+}
+
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+    s = __fadd_rn(a, b);
+    const float bb = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+constexpr uint32_t RENDER_WARPS = 8;        // warps per CTA
+constexpr uint32_t SM_ROW = 36;             // padded row of the warp tile (floats)
+constexpr uint32_t SM_WARP = 32 * SM_ROW;   // floats per warp tile
+
+// The render pass. Template arguments select the interpolation, whether the
+// channel-controller path is compiled in (the reference builds two pipelines
+// for the same reason, shaders/render.wgsl:36-43), strict rounding, and the
+// mix arithmetic.
+template <int INTERP, bool CHAN, bool STRICT, int MIX>
+__global__ void __launch_bounds__(RENDER_WARPS * 32)
+k_render(RenderArgs a) {
+    extern __shared__ float4 smem4[];
+    float* sm = reinterpret_cast<float*>(smem4) + (threadIdx.x >> 5) * SM_WARP;
+    const uint32_t lane = lane_id();
+    const uint32_t gw = blockIdx.x * RENDER_WARPS + (threadIdx.x >> 5);
+    const uint32_t tw = gridDim.x * RENDER_WARPS;
+    const uint32_t n = a.st->live_render;
+    const uint32_t nbatch = (n + 31u) >> 5;
+    const uint32_t samples = a.block_frames * 2u;
+    const uint32_t chan_active = CHAN ? a.ctl->chan_active : 0u;
+    float* __restrict__ part = a.partial + (size_t)gw * samples;
+    float* __restrict__ part_c = MIX ? a.partial_c + (size_t)gw * samples : nullptr;
+    const uint32_t cap = a.cap;
+
+    for (uint32_t b = gw; b < nbatch; b += tw) {
+        const uint32_t vi = (b << 5) + lane;
+        const bool live = vi < n;
+        VoiceRegs v;
+        v.stage = ENV_DEAD;
+        v.phase = 0; v.step = 0; v.base_step = 0;
+        v.base = 0; v.len = 1; v.ls = 0; v.le = 1;
+        v.level = 0.0f; v.gl = v.gr = v.bgl = v.bgr = 0.0f; v.z1 = v.z2 = 0.0f;
+        v.ar = v.ae = v.dc = v.dt = v.sus = v.rc = v.b0 = v.b1 = v.a1 = v.a2 = 0.0f;
+        v.filt = false; v.loop_en = false; v.lur = false;
+        v.params_base = 0; v.variant = 0; v.born = 0; v.born_gate = 0;
+        v.slot = 0; v.ordinal = 0; v.start_rel = 0; v.stop_rel = 0; v.channel = 0;
+        if (live) {
+            const uint32_t* P = a.pool + vi;
+            v.phase = ((uint64_t)P[F_PHASE_HI * cap] << 32) | P[F_PHASE_LO * cap];
+            v.base_step = ((uint64_t)P[F_STEP_HI * cap] << 32) | P[F_STEP_LO * cap];
+            v.step = v.base_step;
+            v.base = P[F_SMP_BASE * cap];
+            v.len = P[F_SMP_LEN * cap];
+            v.ls = P[F_LOOP_START * cap];
+            v.le = P[F_LOOP_END * cap];
+            const uint32_t fl = P[F_FLAGS * cap];
+            v.loop_en = (fl & KC_VF_LOOP) != 0u;
+            v.lur = (fl & KC_VF_LOOP_UNTIL_RELEASE) != 0u;
+            v.stage = P[F_ENV_STAGE * cap];
+            v.level = __uint_as_float(P[F_ENV_LEVEL * cap]);
+            v.bgl = __uint_as_float(P[F_GAIN_L * cap]);
+            v.bgr = __uint_as_float(P[F_GAIN_R * cap]);
+            v.gl = v.bgl; v.gr = v.bgr;
+            v.z1 = __uint_as_float(P[F_FILT_Z1 * cap]);
+            v.z2 = __uint_as_float(P[F_FILT_Z2 * cap]);
+            v.params_base = P[F_PARAMS * cap];
+            v.slot = P[F_GATE_SLOT * cap];
+            v.ordinal = P[F_ORDINAL * cap];
+            v.start_rel = P[F_START_REL * cap];
+            v.born = P[F_BORN_VARIANT * cap];
+            v.stop_rel = P[F_STOP_REL * cap];
+            v.variant = v.born ? v.born - 1u : 0u;
+            v.channel = (v.slot >> 7) & 15u;
+            v.born_gate = v.start_rel / a.gate_frames;
+            if (v.params_base >= a.params_per) {
+                atomicOr(&a.st->error, ERR_PARAMS_RANGE);
+                v.params_base = 0;
+            }
+            load_params(v, a, v.variant);
+        }
+        const bool first = b == gw;
+
+        for (uint32_t f0 = 0; f0 < a.block_frames; f0 += MIX_TILE) {
+            if (f0 % a.gate_frames == 0u && v.stage != ENV_DEAD) {
+                const uint32_t gt = f0 / a.gate_frames;
+                // Note-off gate (src/cpu.rs:450-456).
+                if (v.stage < ENV_RELEASE && __ldg(a.gates + (size_t)gt * KC_GATE_SLOTS + v.slot) >= v.ordinal) {
+                    v.stage = ENV_RELEASE;
+                    v.level = fminf(v.level, 1.0f);
+                }
+                if (CHAN && chan_active) {
+                    // Channel controller path (src/cpu.rs:458-487).
+                    const uint4 row = __ldg(reinterpret_cast<const uint4*>(a.chan) + gt * KC_BEND_CHANNELS + v.channel);
+                    if (chan_active & 1u) v.step = scale_step(v.base_step, row.x);
+                    if (chan_active & 2u) {
+                        v.gl = __fmul_rn(v.bgl, __uint_as_float(row.y));
+                        v.gr = __fmul_rn(v.bgr, __uint_as_float(row.z));
+                    }
+                    if (chan_active & 4u) {
+                        const bool born_here = v.born != 0u && gt <= v.born_gate;
+                        if (row.w != v.variant && !born_here) {
+                            v.variant = row.w;
+                            load_params(v, a, v.variant);
+                        }
+                    }
+                }
+            }
+            const bool looping = v.loop_en && !(v.lur && v.stage >= ENV_RELEASE);
+#pragma unroll 4
+            for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                const uint32_t f = f0 + i;
+                float yl = 0.0f, yr = 0.0f;
+                if (v.stage != ENV_DEAD && f >= v.start_rel) {
+                    const float y = voice_frame<INTERP, STRICT>(v, a, f, looping);
+                    yl = __fmul_rn(y, v.gl);
+                    yr = __fmul_rn(y, v.gr);
+                }
+                sm[(2u * i) * SM_ROW + lane] = yl;
+                sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+            }
+            __syncwarp();
+            // Lane l folds row l (one output slot over the warp's 32 voices).
+            const float4* row = reinterpret_cast<const float4*>(sm + lane * SM_ROW);
+            float4 q[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) q[c] = row[c];
+            __syncwarp();
+            const uint32_t j = f0 * 2u + lane;
+            if (MIX == KC_MIX_F32_TREE) {
+                float r[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) r[c] = __fadd_rn(__fadd_rn(q[c].x, q[c].y), __fadd_rn(q[c].z, q[c].w));
+                const float sum = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                                            __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+                part[j] = first ? sum : __fadd_rn(part[j], sum);
+            } else {
+                // Compensated: sequential two-sum over the row with carries.
+                float s = q[0].x, e = 0.0f, t, err;
+                const float* qq = reinterpret_cast<const float*>(q);
+#pragma unroll
+                for (int c = 1; c < 32; ++c) {
+                    two_sum(s, qq[c], t, err);
+                    s = t;
+                    e = __fadd_rn(e, err);
+                }
+                if (first) {
+                    part[j] = s;
+                    part_c[j] = e;
+                } else {
+                    two_sum(part[j], s, t, err);
+                    part[j] = t;
+                    part_c[j] = __fadd_rn(__fadd_rn(part_c[j], e), err);
+                }
+            }
+        }
+
+        if (live) {
+            uint32_t* P = a.pool + vi;
+            P[F_PHASE_LO * cap] = (uint32_t)v.phase;
+            P[F_PHASE_HI * cap] = (uint32_t)(v.phase >> 32);
+            P[F_ENV_STAGE * cap] = v.stage;
+            P[F_ENV_LEVEL * cap] = __float_as_uint(v.level);
+            P[F_FILT_Z1 * cap] = __float_as_uint(v.z1);
+            P[F_FILT_Z2 * cap] = __float_as_uint(v.z2);
+            P[F_START_REL * cap] = 0u;
+            P[F_BORN_VARIANT * cap] = 0u;
+            P[F_STOP_REL * cap] = 0u;
+        }
+    }
+}
+
+// Fold the warps' partial slices into the output block in a fixed order:
+// warp k of the CTA sums slices k, k+8, ... for 32 consecutive samples, then
+// warp 0 adds the eight in order. Also records max |out| for BlockStats::peak.
+template <int MIX>
+__global__ void __launch_bounds__(256) k_reduce(const float* __restrict__ partial,
+                                                const float* __restrict__ partial_c,
+                                                float* __restrict__ out, DevState* st,
+                                                uint32_t samples) {
+    __shared__ float red[8][32];
+    __shared__ float redc[8][32];
+    const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
+    const uint32_t j = blockIdx.x * 32u + lane;
+    const uint32_t nw = st->active_warps;
+    float s = 0.0f, e = 0.0f;
+    if (j < samples) {
+        for (uint32_t k = w; k < nw; k += 8u) {
+            const size_t o = (size_t)k * samples + j;
+            if (MIX == KC_MIX_F32_TREE) {
+                s = __fadd_rn(s, __ldcs(partial + o));
+            } else {
+                float t, err;
+                two_sum(s, __ldcs(partial + o), t, err);
+                s = t;
+                e = __fadd_rn(__fadd_rn(e, __ldcs(partial_c + o)), err);
+            }
+        }
+    }
+    red[w][lane] = s;
+    redc[w][lane] = e;
+    __syncthreads();
+    if (w == 0 && j < samples) {
+        float tot = red[0][lane], c = redc[0][lane];
+        for (int k = 1; k < 8; ++k) {
+            if (MIX == KC_MIX_F32_TREE) {
+                tot = __fadd_rn(tot, red[k][lane]);
+            } else {
+                float t, err;
+                two_sum(tot, red[k][lane], t, err);
+                tot = t;
+                c = __fadd_rn(__fadd_rn(c, redc[k][lane]), err);
+            }
+        }
+        if (MIX != KC_MIX_F32_TREE) tot = __fadd_rn(tot, c);
+        out[j] = tot;
+        // |x| of a finite float orders like its bit pattern.
+        atomicMax(&st->peak_bits, __float_as_uint(fabsf(tot)));
+    }
+}
+
+}  // namespace kc

@@ -1,0 +1,638 @@
+// synth.cu -- host orchestrator and C ABI of the B200 synthesis backend.
+//
+// One kc_synth is one Backend (src/backend.rs:22-58): it owns the device copy
+// of the sample pool and params tables, a double-buffered structure-of-arrays
+// voice pool in HBM, one CUDA stream, and pinned staging for the per-block
+// inputs. A block is a fixed sequence of kernel launches whose counts all live
+// on the device (DevState), so nothing comes back to the host between the
+// steal, spawn, render, mix and compaction passes; kc_render then reads the
+// stereo block and the state words back in one copy.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "pool_ops.cuh"
+#include "render.cuh"
+
+using namespace kc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define KC_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(KC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int N_TIMERS = 5;
+const char* kPassNames[N_TIMERS] = {"steal", "spawn", "render", "reduce", "compact"};
+
+uint32_t max_steal_of(const kc_config& c) {
+    const uint64_t n = (uint64_t)c.max_voices * c.max_steal_percent / 100;
+    const uint32_t v = (uint32_t)n;
+    return v > 1 ? v : 1;
+}
+
+uint32_t clz32(uint32_t v) { return v ? (uint32_t)__builtin_clz(v) : 32u; }
+
+// SortKeyLayout::plan, src/gpu/mod.rs:77-105.
+SortLayout plan_sort(uint32_t n_regions, uint32_t max_len) {
+    SortLayout L{};
+    L.dead_region = std::max<uint32_t>(n_regions, 1);
+    const uint32_t region_bits = 32 - clz32(L.dead_region);
+    const uint32_t stage_bits = 3;
+    const uint32_t len_bits = 32 - clz32(std::max<uint32_t>(max_len, 1));
+    const uint32_t room = region_bits + stage_bits >= 32 ? 0 : 32 - (region_bits + stage_bits);
+    const uint32_t phase_bits = std::min(room, len_bits);
+    L.phase_shift = len_bits > phase_bits ? len_bits - phase_bits : 0;
+    L.phase_mask = phase_bits >= 32 ? 0xFFFFFFFFu : ((1u << phase_bits) - 1u);
+    L.bits = region_bits + stage_bits + phase_bits;
+    L.region_shift = phase_bits + stage_bits;
+    L.stage_shift = phase_bits;
+    return L;
+}
+
+template <int I, bool C, bool S, int M>
+void* render_fn() {
+    return reinterpret_cast<void*>(&k_render<I, C, S, M>);
+}
+
+// Table of render instantiations indexed [interp][chan][strict][mix].
+void* render_table(uint32_t interp, bool chan, bool strict, uint32_t mix) {
+    static void* t[3][2][2][2] = {
+        {{{render_fn<0, false, false, 0>(), render_fn<0, false, false, 1>()},
+          {render_fn<0, false, true, 0>(), render_fn<0, false, true, 1>()}},
+         {{render_fn<0, true, false, 0>(), render_fn<0, true, false, 1>()},
+          {render_fn<0, true, true, 0>(), render_fn<0, true, true, 1>()}}},
+        {{{render_fn<1, false, false, 0>(), render_fn<1, false, false, 1>()},
+          {render_fn<1, false, true, 0>(), render_fn<1, false, true, 1>()}},
+         {{render_fn<1, true, false, 0>(), render_fn<1, true, false, 1>()},
+          {render_fn<1, true, true, 0>(), render_fn<1, true, true, 1>()}}},
+        {{{render_fn<2, false, false, 0>(), render_fn<2, false, false, 1>()},
+          {render_fn<2, false, true, 0>(), render_fn<2, false, true, 1>()}},
+         {{render_fn<2, true, false, 0>(), render_fn<2, true, false, 1>()},
+          {render_fn<2, true, true, 0>(), render_fn<2, true, true, 1>()}}},
+    };
+    return t[interp][chan ? 1 : 0][strict ? 1 : 0][mix ? 1 : 0];
+}
+
+}  // namespace
+
+struct kc_synth {
+    kc_config cfg{};
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+
+    uint32_t cap = 0;           // pool slots, padded to 32
+    uint32_t tiles = 0;         // gate tiles per block
+    uint32_t params_per = 0;    // entries per params variant
+    uint32_t n_slots = 0;       // params variant slots
+    uint64_t pcm_len = 0;
+    SortLayout sort{};
+
+    // device buffers
+    uint32_t* pool[2] = {nullptr, nullptr};
+    int parity = 0;
+    int16_t* pcm = nullptr;
+    kc_region_params* params = nullptr;
+    uint32_t* gates = nullptr;
+    uint32_t* chan = nullptr;
+    kc_spawn_cmd* cmds = nullptr;
+    uint32_t cmds_cap = 0;
+    float* out = nullptr;
+    float* partial = nullptr;
+    float* partial_c = nullptr;
+    DevState* st = nullptr;
+    BlockCtl* ctl = nullptr;
+    uint32_t* sel_hist = nullptr;
+    uint32_t* counts = nullptr;
+    uint32_t* total = nullptr;
+    uint32_t* keys[2] = {nullptr, nullptr};
+    uint32_t* idx[2] = {nullptr, nullptr};
+
+    // launch geometry
+    uint32_t render_ctas = 0, render_warps = 0;
+    size_t render_smem = 0;
+    uint32_t pool_ctas = 0;     // grid-stride passes
+    uint32_t compact_ctas = 0;  // chunked passes (compaction, sort)
+
+    // pinned host staging
+    uint32_t* h_gates = nullptr;
+    uint32_t* h_chan = nullptr;
+    kc_spawn_cmd* h_cmds = nullptr;
+    uint32_t h_cmds_cap = 0;
+    float* h_out = nullptr;
+    DevState* h_st = nullptr;
+
+    uint32_t want = 0;
+    bool bend = false, gain = false, variant = false;
+
+    // host mirror of BlockStats
+    kc_block_stats stats{};
+
+    bool profile = false;
+    cudaEvent_t ev[N_TIMERS + 1] = {};
+    double last_ms[N_TIMERS] = {};
+    bool have_timings = false;
+};
+
+namespace {
+
+void free_all(kc_synth* s) {
+    if (!s) return;
+    cudaFree(s->pool[0]);
+    cudaFree(s->pool[1]);
+    cudaFree(s->pcm);
+    cudaFree(s->params);
+    cudaFree(s->gates);
+    cudaFree(s->chan);
+    cudaFree(s->cmds);
+    cudaFree(s->out);
+    cudaFree(s->partial);
+    cudaFree(s->partial_c);
+    cudaFree(s->st);
+    cudaFree(s->ctl);
+    cudaFree(s->sel_hist);
+    cudaFree(s->counts);
+    cudaFree(s->total);
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(s->keys[i]);
+        cudaFree(s->idx[i]);
+    }
+    cudaFreeHost(s->h_gates);
+    cudaFreeHost(s->h_chan);
+    cudaFreeHost(s->h_cmds);
+    cudaFreeHost(s->h_out);
+    cudaFreeHost(s->h_st);
+    for (auto& e : s->ev)
+        if (e) cudaEventDestroy(e);
+    if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// Config::validate (src/config.rs:412-525), the part the backend reads, plus
+// this backend's own tiling constraints.
+int validate(const kc_config& c) {
+    if (c.sample_rate < 8000 || c.sample_rate > 768000) return fail(KC_ERR_INVALID, "sample_rate out of range");
+    if (c.block_frames == 0 || c.block_frames % MIX_TILE != 0 || c.block_frames > 65535)
+        return fail(KC_ERR_INVALID, "block_frames must be a non-zero multiple of 16, at most 65535");
+    if (c.gate_frames == 0 || c.gate_frames % MIX_TILE != 0 || c.block_frames % c.gate_frames != 0)
+        return fail(KC_ERR_INVALID, "gate_frames must be a multiple of 16 that divides block_frames");
+    if (c.max_voices == 0) return fail(KC_ERR_INVALID, "max_voices must be non-zero");
+    if (c.steal_fade_frames == 0 || c.steal_fade_frames >= c.block_frames)
+        return fail(KC_ERR_INVALID, "steal_fade_frames must be in 1..block_frames");
+    if (c.max_steal_percent == 0 || c.max_steal_percent > 100)
+        return fail(KC_ERR_INVALID, "max_steal_percent must be in 1..=100");
+    if (c.steal_rule > 2 || c.admit_rule > 1 || c.interpolation > 2 || c.decay_curve > 1 ||
+        c.release_curve > 1 || c.mix_mode > 1)
+        return fail(KC_ERR_INVALID, "unknown enum value in config");
+    if (c.max_param_variants == 0 || c.max_param_variants > 64)
+        return fail(KC_ERR_INVALID, "max_param_variants must be in 1..=64");
+    return KC_OK;
+}
+
+// Enqueue one block on the stream. All inputs are device pointers.
+int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, bool bend, bool gain,
+                  bool variant, const kc_spawn_cmd* d_cmds, uint32_t n_cmds, float* d_out) {
+    cudaStream_t q = s->stream;
+    const kc_config& c = s->cfg;
+    const uint32_t chan_active = (bend ? 1u : 0u) | (gain ? 2u : 0u) | (variant ? 4u : 0u);
+
+    PoolArgs pa{};
+    pa.pool = s->pool[s->parity];
+    pa.pool_out = s->pool[s->parity ^ 1];
+    pa.cap = s->cap;
+    pa.st = s->st;
+    pa.ctl = s->ctl;
+    pa.max_voices = c.max_voices;
+    pa.max_steal = max_steal_of(c);
+    pa.steal_rule = c.steal_rule;
+    pa.admit_rule = c.admit_rule;
+    const uint32_t span = c.block_frames > c.steal_fade_frames ? c.block_frames - c.steal_fade_frames : 1;
+    pa.steal_span = std::max<uint32_t>(span, 1);
+    pa.render_warps = s->render_warps;
+
+    if (s->profile) cudaEventRecord(s->ev[0], q);
+    k_admit<<<1, 256, 0, q>>>(pa, s->sel_hist, s->ctl, n_cmds, chan_active);
+    // ---- 1. steal ----
+    if (c.steal_rule != KC_STEAL_DROP_NEW) {
+        for (uint32_t r = 0; r < SEL_ROUNDS; ++r) {
+            k_select_hist<<<s->pool_ctas, 256, 0, q>>>(pa, s->sel_hist, r);
+            k_select_refine<<<1, 256, 0, q>>>(pa, s->sel_hist, r);
+        }
+        k_mark_stolen<<<s->pool_ctas, 256, 0, q>>>(pa);
+    }
+    if (s->profile) cudaEventRecord(s->ev[1], q);
+    // ---- 2. spawn ----
+    k_spawn<<<s->pool_ctas, 256, 0, q>>>(pa, d_cmds);
+    if (s->profile) cudaEventRecord(s->ev[2], q);
+    // ---- 3. render ----
+    RenderArgs ra{};
+    ra.pool = pa.pool;
+    ra.cap = s->cap;
+    ra.pcm = s->pcm;
+    ra.pcm_len = (uint32_t)std::min<uint64_t>(s->pcm_len, 0xFFFFFFFFull);
+    ra.params = s->params;
+    ra.params_per = s->params_per;
+    ra.n_slots = s->n_slots;
+    ra.gates = d_gates;
+    ra.chan = d_chan;
+    ra.ctl = s->ctl;
+    ra.st = s->st;
+    ra.partial = s->partial;
+    ra.partial_c = s->partial_c;
+    ra.block_frames = c.block_frames;
+    ra.gate_frames = c.gate_frames;
+    ra.fade = c.steal_fade_frames;
+    ra.env_floor = c.env_floor;
+    ra.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
+    ra.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
+    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode);
+    void* args[] = {&ra};
+    KC_CUDA(cudaLaunchKernel(fn, dim3(s->render_ctas), dim3(RENDER_WARPS * 32), args, s->render_smem, q));
+    if (s->profile) cudaEventRecord(s->ev[3], q);
+    // ---- 4. reduce ----
+    const uint32_t samples = c.block_frames * 2;
+    if (c.mix_mode == KC_MIX_F32_TREE)
+        k_reduce<0><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
+    else
+        k_reduce<1><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
+    if (s->profile) cudaEventRecord(s->ev[4], q);
+    // ---- 5. compact (and sort) ----
+    k_compact_count<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
+    k_scan_counts<<<1, 1024, 0, q>>>(s->counts, s->compact_ctas, s->total);
+    k_commit<<<1, 1, 0, q>>>(s->st, s->total);
+    if (!c.sort_voices) {
+        k_compact_scatter<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
+    } else {
+        const uint32_t passes = (s->sort.bits + 7) / 8;
+        const uint32_t G = s->compact_ctas;
+        int cur = 0;
+        for (uint32_t p = 0; p < passes; ++p) {
+            const uint32_t shift = 8 * p;
+            const uint32_t* kin = p == 0 ? nullptr : s->keys[cur];
+            const uint32_t* iin = p == 0 ? nullptr : s->idx[cur];
+            k_sort_count<<<G, 256, 0, q>>>(pa, s->sort, kin, shift, s->counts);
+            k_scan_counts<<<1, 1024, 0, q>>>(s->counts, 256 * G, s->total + 1);
+            k_sort_scatter<<<G, 256, 0, q>>>(pa, s->sort, kin, iin, s->keys[cur ^ 1], s->idx[cur ^ 1], shift,
+                                             s->counts);
+            cur ^= 1;
+        }
+        k_sort_gather<<<s->pool_ctas, 256, 0, q>>>(pa, s->idx[cur]);
+    }
+    if (s->profile) cudaEventRecord(s->ev[5], q);
+    KC_CUDA(cudaGetLastError());
+    s->parity ^= 1;
+    return KC_OK;
+}
+
+uint32_t launches_per_block(const kc_synth* s) {
+    uint32_t n = 1;                                                       // admit
+    if (s->cfg.steal_rule != KC_STEAL_DROP_NEW) n += 2 * SEL_ROUNDS + 1;  // select + mark
+    n += 1 + 1 + 1;                                                       // spawn, render, reduce
+    n += 3;                                                               // count, scan, commit
+    if (!s->cfg.sort_voices) n += 1;
+    else n += 3 * ((s->sort.bits + 7) / 8) + 1;
+    return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* kc_last_error(void) { return g_err.c_str(); }
+
+int kc_config_default(kc_config* c) {
+    if (!c) return fail(KC_ERR_INVALID, "null config");
+    std::memset(c, 0, sizeof(*c));
+    c->sample_rate = 48000;
+    c->block_frames = 4096;
+    c->gate_frames = 32;
+    c->max_voices = 1u << 20;
+    c->max_steal_percent = 25;
+    c->steal_fade_frames = 96;
+    c->steal_rule = KC_STEAL_QUIETEST;
+    c->admit_rule = KC_ADMIT_LOUDEST;
+    c->interpolation = KC_INTERP_LINEAR;
+    c->decay_curve = KC_CURVE_EXPONENTIAL;
+    c->release_curve = KC_CURVE_EXPONENTIAL;
+    c->env_floor = 1.0e-5f;
+    c->sort_voices = 1;
+    c->max_param_variants = 32;
+    c->mix_mode = KC_MIX_F32_TREE;
+    c->strict_fp = 1;
+    c->device = 0;
+    return KC_OK;
+}
+
+uint32_t kc_pool_slots(const kc_config* c) {
+    const uint64_t s = (uint64_t)c->max_voices + max_steal_of(*c);
+    return s > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)s;
+}
+
+int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len,
+                    const kc_region_params* params, uint32_t params_len, uint32_t n_regions,
+                    uint32_t max_sample_len, kc_synth** out) {
+    if (!cfg || !out) return fail(KC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (int rc = validate(*cfg)) return rc;
+    if (params_len == 0 || !params) return fail(KC_ERR_INVALID, "params table is empty");
+    if (pool_len && !pool) return fail(KC_ERR_INVALID, "null sample pool");
+    const uint64_t slots = kc_pool_slots(cfg);
+    if (slots > 0x7FFFFFE0ull) return fail(KC_ERR_INVALID, "pool slots exceed 2^31");
+
+    kc_synth* s = new kc_synth();
+    s->cfg = *cfg;
+    s->device = (int)cfg->device;
+    auto bail = [&](int rc) {
+        free_all(s);
+        delete s;
+        return rc;
+    };
+#define KC_TRY(call)                                                                      \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return bail(fail(e_ == cudaErrorMemoryAllocation ? KC_ERR_OOM : KC_ERR_CUDA,  \
+                             std::string(#call) + ": " + cudaGetErrorString(e_)));        \
+    } while (0)
+
+    KC_TRY(cudaSetDevice(s->device));
+    KC_TRY(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device));
+    KC_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+
+    s->cap = (uint32_t)((slots + 31) & ~31ull);
+    s->tiles = cfg->block_frames / cfg->gate_frames;
+    s->params_per = params_len;
+    s->n_slots = cfg->max_param_variants;
+    s->pcm_len = pool_len;
+    s->sort = plan_sort(n_regions, max_sample_len);
+
+    // Launch geometry: the render grid is every resident CTA of the device,
+    // and the partial buffer has one slice per render warp.
+    s->render_smem = (size_t)RENDER_WARPS * SM_WARP * sizeof(float);
+    void* fn = render_table(cfg->interpolation, true, cfg->strict_fp != 0, cfg->mix_mode);
+    KC_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->render_smem));
+    for (int ch = 0; ch < 2; ++ch) {
+        void* f2 = render_table(cfg->interpolation, ch != 0, cfg->strict_fp != 0, cfg->mix_mode);
+        KC_TRY(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->render_smem));
+    }
+    int per_sm = 0;
+    KC_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, RENDER_WARPS * 32, s->render_smem));
+    per_sm = std::max(per_sm, 1);
+    s->render_ctas = (uint32_t)(s->sms * per_sm);
+    s->render_warps = s->render_ctas * RENDER_WARPS;
+    s->pool_ctas = (uint32_t)s->sms * 4;
+    s->compact_ctas = (uint32_t)s->sms * 2;
+
+    const size_t pool_words = (size_t)VOICE_FIELDS * s->cap;
+    KC_TRY(cudaMalloc(&s->pool[0], pool_words * 4));
+    KC_TRY(cudaMalloc(&s->pool[1], pool_words * 4));
+    KC_TRY(cudaMalloc(&s->pcm, std::max<uint64_t>(pool_len, 1) * 2 + 64));
+    if (pool_len) KC_TRY(cudaMemcpy(s->pcm, pool, pool_len * 2, cudaMemcpyHostToDevice));
+    const size_t per_bytes = (size_t)params_len * sizeof(kc_region_params);
+    KC_TRY(cudaMalloc(&s->params, per_bytes * s->n_slots));
+    // Every slot starts as a copy of the bank's table, which is what
+    // CpuSynth::params_of falls back to for a variant never uploaded.
+    for (uint32_t v = 0; v < s->n_slots; ++v)
+        KC_TRY(cudaMemcpy((char*)s->params + v * per_bytes, params, per_bytes, cudaMemcpyHostToDevice));
+    const size_t gate_words = (size_t)s->tiles * KC_GATE_SLOTS;
+    const size_t chan_words = (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS;
+    KC_TRY(cudaMalloc(&s->gates, gate_words * 4));
+    KC_TRY(cudaMalloc(&s->chan, chan_words * 4));
+    KC_TRY(cudaMemset(s->gates, 0, gate_words * 4));
+    KC_TRY(cudaMemset(s->chan, 0, chan_words * 4));
+    s->cmds_cap = 4096;
+    KC_TRY(cudaMalloc(&s->cmds, (size_t)s->cmds_cap * sizeof(kc_spawn_cmd)));
+    const size_t samples = (size_t)cfg->block_frames * 2;
+    KC_TRY(cudaMalloc(&s->out, samples * 4));
+    KC_TRY(cudaMalloc(&s->partial, (size_t)s->render_warps * samples * 4));
+    if (cfg->mix_mode != KC_MIX_F32_TREE) KC_TRY(cudaMalloc(&s->partial_c, (size_t)s->render_warps * samples * 4));
+    KC_TRY(cudaMalloc(&s->st, sizeof(DevState)));
+    KC_TRY(cudaMemset(s->st, 0, sizeof(DevState)));
+    KC_TRY(cudaMalloc(&s->ctl, sizeof(BlockCtl)));
+    KC_TRY(cudaMalloc(&s->sel_hist, SEL_ROUNDS * 256 * 4));
+    KC_TRY(cudaMalloc(&s->counts, (size_t)256 * s->compact_ctas * 4));
+    KC_TRY(cudaMalloc(&s->total, 16));
+    if (cfg->sort_voices) {
+        for (int i = 0; i < 2; ++i) {
+            KC_TRY(cudaMalloc(&s->keys[i], (size_t)s->cap * 4));
+            KC_TRY(cudaMalloc(&s->idx[i], (size_t)s->cap * 4));
+        }
+    }
+    KC_TRY(cudaMallocHost(&s->h_gates, gate_words * 4));
+    KC_TRY(cudaMallocHost(&s->h_chan, chan_words * 4));
+    std::memset(s->h_gates, 0, gate_words * 4);
+    std::memset(s->h_chan, 0, chan_words * 4);
+    s->h_cmds_cap = 4096;
+    KC_TRY(cudaMallocHost(&s->h_cmds, (size_t)s->h_cmds_cap * sizeof(kc_spawn_cmd)));
+    KC_TRY(cudaMallocHost(&s->h_out, samples * 4));
+    KC_TRY(cudaMallocHost(&s->h_st, sizeof(DevState)));
+    for (auto& e : s->ev) KC_TRY(cudaEventCreate(&e));
+    KC_TRY(cudaDeviceSynchronize());
+#undef KC_TRY
+    *out = s;
+    return KC_OK;
+}
+
+void kc_synth_destroy(kc_synth* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_all(s);
+    delete s;
+}
+
+int kc_set_gates(kc_synth* s, const uint32_t* rows, size_t n) {
+    if (!s || (!rows && n)) return fail(KC_ERR_INVALID, "null argument");
+    if (n != (size_t)s->tiles * KC_GATE_SLOTS)
+        return fail(KC_ERR_INVALID, "gate rows: expected tiles * 2048 words");
+    std::memcpy(s->h_gates, rows, n * 4);
+    return KC_OK;
+}
+
+int kc_set_channels(kc_synth* s, const uint32_t* rows, size_t n, int bend, int gain, int variant) {
+    if (!s || (!rows && n)) return fail(KC_ERR_INVALID, "null argument");
+    if (n != (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS)
+        return fail(KC_ERR_INVALID, "channel rows: expected tiles * 64 words");
+    std::memcpy(s->h_chan, rows, n * 4);
+    s->bend = bend != 0;
+    s->gain = gain != 0;
+    s->variant = variant != 0;
+    return KC_OK;
+}
+
+int kc_set_params_variant(kc_synth* s, uint32_t index, const kc_region_params* data, size_t n) {
+    if (!s) return fail(KC_ERR_INVALID, "null synth");
+    if (index == 0) return KC_OK;  // the bank's own table (src/cpu.rs:314-316)
+    if (n != s->params_per)
+        return fail(KC_ERR_INVALID, "params variant " + std::to_string(index) + " has " + std::to_string(n) +
+                                        " entries, expected " + std::to_string(s->params_per));
+    if (index >= s->n_slots) return fail(KC_ERR_INVALID, "params variant is past the configured maximum");
+    cudaSetDevice(s->device);
+    KC_CUDA(cudaStreamSynchronize(s->stream));
+    KC_CUDA(cudaMemcpy((char*)s->params + (size_t)index * n * sizeof(kc_region_params), data,
+                       n * sizeof(kc_region_params), cudaMemcpyHostToDevice));
+    return KC_OK;
+}
+
+int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n) {
+    if (!s || (!cmds && n)) return fail(KC_ERR_INVALID, "null argument");
+    if (n > 0x7FFFFFFFull) return fail(KC_ERR_INVALID, "too many spawn commands");
+    // The CPU backend indexes these tables directly and would panic on a bad
+    // index; reject them here instead of reading out of bounds on the device.
+    for (size_t i = 0; i < n; ++i) {
+        if (cmds[i].params >= s->params_per) return fail(KC_ERR_INVALID, "spawn command params index out of range");
+        if (cmds[i].gate_slot >= KC_GATE_SLOTS) return fail(KC_ERR_INVALID, "spawn command gate_slot out of range");
+    }
+    if (n > s->h_cmds_cap) {
+        cudaSetDevice(s->device);
+        KC_CUDA(cudaStreamSynchronize(s->stream));
+        uint32_t nc = std::max<uint32_t>(s->h_cmds_cap, 1);
+        while (nc < n) nc *= 2;
+        cudaFreeHost(s->h_cmds);
+        s->h_cmds = nullptr;
+        s->h_cmds_cap = 0;
+        if (cudaMallocHost(&s->h_cmds, (size_t)nc * sizeof(kc_spawn_cmd)) != cudaSuccess)
+            return fail(KC_ERR_OOM, "pinned spawn staging");
+        s->h_cmds_cap = nc;
+    }
+    if (n) std::memcpy(s->h_cmds, cmds, n * sizeof(kc_spawn_cmd));
+    s->want = (uint32_t)n;
+    return KC_OK;
+}
+
+int kc_render(kc_synth* s, float* out, size_t n) {
+    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
+    const size_t samples = (size_t)s->cfg.block_frames * 2;
+    if (n != samples) return fail(KC_ERR_INVALID, "output must be block_frames * 2 samples");
+    cudaSetDevice(s->device);
+    cudaStream_t q = s->stream;
+    if (s->want > s->cmds_cap) {
+        KC_CUDA(cudaStreamSynchronize(q));
+        uint32_t nc = std::max<uint32_t>(s->cmds_cap, 1);
+        while (nc < s->want) nc *= 2;
+        cudaFree(s->cmds);
+        s->cmds = nullptr;
+        s->cmds_cap = 0;
+        if (cudaMalloc(&s->cmds, (size_t)nc * sizeof(kc_spawn_cmd)) != cudaSuccess)
+            return fail(KC_ERR_OOM, "device spawn buffer");
+        s->cmds_cap = nc;
+    }
+    const size_t gate_words = (size_t)s->tiles * KC_GATE_SLOTS;
+    const size_t chan_words = (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS;
+    KC_CUDA(cudaMemcpyAsync(s->gates, s->h_gates, gate_words * 4, cudaMemcpyHostToDevice, q));
+    KC_CUDA(cudaMemcpyAsync(s->chan, s->h_chan, chan_words * 4, cudaMemcpyHostToDevice, q));
+    if (s->want)
+        KC_CUDA(cudaMemcpyAsync(s->cmds, s->h_cmds, (size_t)s->want * sizeof(kc_spawn_cmd),
+                                cudaMemcpyHostToDevice, q));
+    if (int rc = enqueue_block(s, s->gates, s->chan, s->bend, s->gain, s->variant, s->cmds, s->want, s->out))
+        return rc;
+    KC_CUDA(cudaMemcpyAsync(s->h_out, s->out, samples * 4, cudaMemcpyDeviceToHost, q));
+    KC_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, q));
+    KC_CUDA(cudaStreamSynchronize(q));
+    std::memcpy(out, s->h_out, samples * 4);
+    s->want = 0;
+    s->stats.active_voices = s->h_st->live;
+    s->stats.stolen = s->h_st->stolen;
+    s->stats.dropped = s->h_st->dropped;
+    uint32_t pb = s->h_st->peak_bits;
+    std::memcpy(&s->stats.peak, &pb, 4);
+    if (s->profile) {
+        for (int i = 0; i < N_TIMERS; ++i) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ev[i], s->ev[i + 1]);
+            s->last_ms[i] = ms;
+        }
+        s->have_timings = true;
+    }
+    if (s->h_st->error)
+        return fail(KC_ERR_DEVICE, "device error word " + std::to_string(s->h_st->error));
+    return KC_OK;
+}
+
+int kc_stats(kc_synth* s, kc_block_stats* out) {
+    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
+    *out = s->stats;
+    return KC_OK;
+}
+
+const char* kc_name(const kc_synth*) { return "cuda-sm100a"; }
+
+int kc_set_profile(kc_synth* s, int on) {
+    if (!s) return fail(KC_ERR_INVALID, "null synth");
+    s->profile = on != 0;
+    s->have_timings = false;
+    return KC_OK;
+}
+
+int kc_timings(kc_synth* s, const char** names, double* ms, size_t cap, size_t* n) {
+    if (!s || !n) return fail(KC_ERR_INVALID, "null argument");
+    *n = 0;
+    if (!s->have_timings) return KC_OK;
+    const size_t k = std::min<size_t>(cap, N_TIMERS);
+    for (size_t i = 0; i < k; ++i) {
+        if (names) names[i] = kPassNames[i];
+        if (ms) ms[i] = s->last_ms[i];
+    }
+    *n = k;
+    return KC_OK;
+}
+
+int kc_enqueue_block_device(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, int bend, int gain,
+                            int variant, const kc_spawn_cmd* d_cmds, uint32_t n_cmds, float* d_out) {
+    if (!s || !d_gates || !d_chan || !d_out || (n_cmds && !d_cmds)) return fail(KC_ERR_INVALID, "null argument");
+    cudaSetDevice(s->device);
+    return enqueue_block(s, d_gates, d_chan, bend != 0, gain != 0, variant != 0, d_cmds, n_cmds, d_out);
+}
+
+int kc_synchronize(kc_synth* s) {
+    if (!s) return fail(KC_ERR_INVALID, "null synth");
+    cudaSetDevice(s->device);
+    KC_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+    KC_CUDA(cudaStreamSynchronize(s->stream));
+    s->stats.active_voices = s->h_st->live;
+    s->stats.stolen = s->h_st->stolen;
+    s->stats.dropped = s->h_st->dropped;
+    uint32_t pb = s->h_st->peak_bits;
+    std::memcpy(&s->stats.peak, &pb, 4);
+    if (s->h_st->error) return fail(KC_ERR_DEVICE, "device error word " + std::to_string(s->h_st->error));
+    return KC_OK;
+}
+
+void* kc_stream(kc_synth* s) { return s ? (void*)s->stream : nullptr; }
+
+int kc_block_launches(kc_synth* s, uint32_t* out) {
+    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
+    *out = launches_per_block(s);
+    return KC_OK;
+}
+
+int kc_read_pool(kc_synth* s, uint32_t* fields, size_t cap_words, uint32_t* live) {
+    if (!s || !live) return fail(KC_ERR_INVALID, "null argument");
+    cudaSetDevice(s->device);
+    KC_CUDA(cudaStreamSynchronize(s->stream));
+    DevState h{};
+    KC_CUDA(cudaMemcpy(&h, s->st, sizeof(h), cudaMemcpyDeviceToHost));
+    *live = h.live;
+    if (cap_words < (size_t)h.live * VOICE_FIELDS) return fail(KC_ERR_INVALID, "buffer too small");
+    if (!h.live) return KC_OK;
+    KC_CUDA(cudaMemcpy2D(fields, (size_t)h.live * 4, s->pool[s->parity], (size_t)s->cap * 4, (size_t)h.live * 4,
+                         VOICE_FIELDS, cudaMemcpyDeviceToHost));
+    return KC_OK;
+}
+
+}  // extern "C"
