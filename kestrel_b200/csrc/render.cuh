@@ -224,6 +224,113 @@ __device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, 
     return y;
 }
 
+// ---- the fast path -----------------------------------------------------------
+// Most 16-frame tiles of most voices need none of the per-frame branches of
+// voice_frame: the voice started before the tile, is not being stolen, and its
+// phase neither wraps a loop nor reaches the sample end inside the tile. For
+// such a tile (checked per lane, taken when the whole warp qualifies) each
+// frame is straight-line code. The envelope step becomes one exactly rounded
+// FMA with per-stage constants:
+//   attack   level*1 + attack_rate      == level + attack_rate
+//   decay    level*decay_coef + 0        == level * decay_coef   (exponential)
+//            level*1 - decay_coef        == level - decay_coef   (linear)
+//   sustain  level*1 + 0                 == level
+//   release  like decay with release_coef
+// (a single rounding of an exact product or sum is the rounding of the
+// reference's own operation), and the stage test "level >= attack_end",
+// "level <= decay_target", "level <= env_floor" becomes sgn*level >= thr with
+// sgn = +-1 (negation is exact). A hit leaves the straight line for the
+// transition code, which is the reference's statement for statement.
+struct EnvStep {
+    float em, ea, sgn, thr;
+};
+
+__device__ __forceinline__ EnvStep env_constants(const VoiceRegs& v, const RenderArgs& a) {
+    EnvStep e;
+    e.em = 1.0f; e.ea = 0.0f; e.sgn = 1.0f; e.thr = __int_as_float(0x7f800000);  // sustain: never
+    if (v.stage == ENV_ATTACK) {
+        e.ea = v.ar; e.thr = v.ae;
+    } else if (v.stage == ENV_DECAY) {
+        if (a.exp_decay) e.em = v.dc; else e.ea = -v.dc;
+        e.sgn = -1.0f; e.thr = -v.dt;
+    } else if (v.stage == ENV_RELEASE) {
+        if (a.exp_release) e.em = v.rc; else e.ea = -v.rc;
+        e.sgn = -1.0f; e.thr = -a.env_floor;
+    }
+    return e;
+}
+
+// The stage transition after a threshold hit (src/cpu.rs:512-549), then the
+// new stage's constants. Returns false when the voice died on this frame.
+__device__ __forceinline__ bool env_transition(VoiceRegs& v, const RenderArgs& a, EnvStep& e) {
+    if (v.stage == ENV_ATTACK) {
+        v.stage = ENV_DECAY;
+        v.level = 1.0f;
+    } else if (v.stage == ENV_DECAY) {
+        if (v.sus <= a.env_floor) {
+            v.stage = ENV_DEAD;
+            v.level = 0.0f;
+        } else {
+            v.stage = ENV_SUSTAIN;
+            v.level = v.sus;
+        }
+    } else if (v.stage == ENV_RELEASE) {
+        v.stage = ENV_DEAD;
+        v.level = 0.0f;
+    }
+    e = env_constants(v, a);
+    return v.stage != ENV_DEAD;
+}
+
+// Can this lane run the tile starting at f0 on the fast path? Idle lanes
+// (no voice, dead, or starting after the tile) qualify trivially.
+__device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a, uint32_t f0, bool looping,
+                                        bool& active) {
+    active = false;
+    if (v.stage == ENV_DEAD || v.start_rel >= f0 + MIX_TILE) return true;
+    if (v.start_rel > f0) return false;                       // starts inside the tile
+    if (v.stop_rel != 0u && v.stop_rel <= f0 + MIX_TILE) return false;  // fade begins inside
+    if (v.step >> 59) return false;
+    const uint64_t end = v.phase + (v.step << 4);
+    if (end < v.phase) return false;
+    const uint32_t hi = (uint32_t)(end >> 32);
+    if (hi == 0xFFFFFFFFu) return false;
+    if (looping ? hi + 1u >= v.le : hi + 1u >= v.len) return false;   // wrap, end or clamp
+    if ((uint64_t)v.base + hi + 1u >= (uint64_t)a.pcm_len) return false;
+    active = true;
+    return true;
+}
+
+template <bool STRICT>
+__device__ __forceinline__ float fast_frame(VoiceRegs& v, const RenderArgs& a, EnvStep& e, bool& active) {
+    // Envelope, exactly rounded in one FMA.
+    v.level = __fmaf_rn(v.level, e.em, e.ea);
+    if (__fmul_rn(e.sgn, v.level) >= e.thr) active = env_transition(v, a, e);
+    // Linear interpolation between two adjacent, in-bounds taps.
+    const uint32_t idx = (uint32_t)(v.phase >> 32);
+    const int16_t* p = a.pcm + (v.base + idx);
+    const float s0 = fmaxf(__fmul_rn((float)__ldg(p), 1.0f / 32767.0f), -1.0f);
+    const float s1 = fmaxf(__fmul_rn((float)__ldg(p + 1), 1.0f / 32767.0f), -1.0f);
+    const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
+    const float s = STRICT ? __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac)) : fmaf(s1 - s0, frac, s0);
+    const float x = __fmul_rn(s, fminf(v.level, 1.0f));
+    float y = x;
+    if (v.filt) {
+        if (STRICT) {
+            const float bx = __fmul_rn(v.b0, x);
+            y = __fadd_rn(bx, v.z1);
+            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
+            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
+        } else {
+            y = fmaf(v.b0, x, v.z1);
+            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
+            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
+        }
+    }
+    v.phase += v.step;
+    return y;
+}
+
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
     const float bb = __fsub_rn(s, a);
@@ -239,7 +346,7 @@ constexpr uint32_t SM_WARP = 32 * SM_ROW;   // floats per warp tile
 // for the same reason, shaders/render.wgsl:36-43), strict rounding, and the
 // mix arithmetic.
 template <int INTERP, bool CHAN, bool STRICT, int MIX>
-__global__ void __launch_bounds__(RENDER_WARPS * 32)
+__global__ void __launch_bounds__(RENDER_WARPS * 32, 3)
 k_render(RenderArgs a) {
     extern __shared__ float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4) + (threadIdx.x >> 5) * SM_WARP;
@@ -328,17 +435,34 @@ k_render(RenderArgs a) {
                 }
             }
             const bool looping = v.loop_en && !(v.lur && v.stage >= ENV_RELEASE);
-#pragma unroll 4
-            for (uint32_t i = 0; i < MIX_TILE; ++i) {
-                const uint32_t f = f0 + i;
-                float yl = 0.0f, yr = 0.0f;
-                if (v.stage != ENV_DEAD && f >= v.start_rel) {
-                    const float y = voice_frame<INTERP, STRICT>(v, a, f, looping);
-                    yl = __fmul_rn(y, v.gl);
-                    yr = __fmul_rn(y, v.gr);
+            bool active = false;
+            const bool ok = INTERP == KC_INTERP_LINEAR && fast_ok(v, a, f0, looping, active);
+            if (__all_sync(0xFFFFFFFFu, ok)) {
+                EnvStep e = env_constants(v, a);
+#pragma unroll
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    float yl = 0.0f, yr = 0.0f;
+                    if (active) {
+                        const float y = fast_frame<STRICT>(v, a, e, active);
+                        yl = __fmul_rn(y, v.gl);
+                        yr = __fmul_rn(y, v.gr);
+                    }
+                    sm[(2u * i) * SM_ROW + lane] = yl;
+                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
                 }
-                sm[(2u * i) * SM_ROW + lane] = yl;
-                sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+            } else {
+#pragma unroll 1
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    const uint32_t f = f0 + i;
+                    float yl = 0.0f, yr = 0.0f;
+                    if (v.stage != ENV_DEAD && f >= v.start_rel) {
+                        const float y = voice_frame<INTERP, STRICT>(v, a, f, looping);
+                        yl = __fmul_rn(y, v.gl);
+                        yr = __fmul_rn(y, v.gr);
+                    }
+                    sm[(2u * i) * SM_ROW + lane] = yl;
+                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                }
             }
             __syncwarp();
             // Lane l folds row l (one output slot over the warp's 32 voices).
