@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 synthesis backend on Kestrel's per-block hot path.
+
+One step is one audio block (4096 frames, 48 kHz stereo) of the Backend
+contract: steal-select, spawn, per-voice render, mix, compact/sort.
+
+Workloads (seeded synthetic stand-ins with the shapes the benchmark
+configurations describe; no public dataset is involved):
+  steal  (default) 200M notes over 120 s, log-normal durations (median 6 s,
+         sigma 0.5) so concurrency exceeds the pool; --max-voices 8,388,608,
+         steal-percent 10. The largest single-GPU configuration and the one
+         that actually sustains 8.4M concurrent voices.
+  black  20M notes over 180 s, 60% of onsets in 1 ms clusters of 1k-50k notes,
+         128 presets, bend/CC7/CC11 every 10 ms; --max-voices 1,048,576.
+  plain  100k notes over 30 s, 1 preset, --max-voices 65,536.
+
+Measurement. A driver (the C++ restatement of src/driver.rs) renders a
+pre-roll until the pool reaches its steady state. Then:
+  e2e    W + K blocks through the C ABI with host buffers (kc_set_gates,
+         kc_set_channels, kc_spawn, kc_render): host->device copies of the
+         block's inputs and the device->host read of the stereo block are
+         inside each timed step; the driver's own preparation is not.
+  value  a clone of the context at the same state (kc_synth_clone) replays
+         the same W + K recorded blocks from HBM (kc_enqueue_block_device),
+         K timed back to back with CUDA events on the context's stream.
+The two renders are checked to be byte-identical.
+
+Metric: voice-samples/s = sum over blocks of (voices rendered x 4096) / time;
+x-realtime = audio seconds / time.
+
+`--impl reference` times the CPU restatement of the reference backend
+(src/cpu.rs, the oracle) on the host's cores over the workload's first
+W + K blocks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PREROLL = {"steal": 64, "black": 48, "plain": 24}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--workload", choices=["steal", "black", "plain"], default="steal")
+    ap.add_argument("--preroll", type=int, default=None)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the cpu_baseline sample")
+    return ap.parse_args(argv)
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---- clocks during the timed region ------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in Path(self.path).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---- roofline ------------------------------------------------------------------------
+
+def render_algorithmic_bytes(n_render: int, block_frames: int, tiles: int) -> int:
+    """Algorithmic bytes of one render launch: each voice's 96-byte slot read
+    and its 36 bytes of state written back, one new i16 sample per voice-frame
+    (2 B at step ~1; the sample bank is L2-resident), and the block's gate and
+    channel rows."""
+    return n_render * (96 + 36 + 2 * block_frames) + tiles * 2048 * 4 + tiles * 64 * 4
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def render_traffic_per_unit() -> float | None:
+    """DRAM bytes (read + write) per voice-sample of the render kernel, from the
+    committed ncu summary of that kernel (profiles/render_traffic.json)."""
+    p = ROOT / "profiles" / "render_traffic.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["dram_bytes_per_voice_sample"])
+        except Exception:
+            return None
+    return None
+
+
+# ---- the CUDA arm ------------------------------------------------------------------
+
+def run_cuda(args, world, rank, local):
+    import torch
+    from kestrel_b200 import host as H
+    from kestrel_b200 import native as N
+    from kestrel_b200.backend import CudaSynth
+
+    torch.cuda.set_device(local)
+    cfg, bs, ms = H.config_workload(args.workload, seed=args.seed + rank)
+    cfg.device = local
+    bank = H.Bank(bs, cfg)
+    drv = H.Driver(cfg, bank, ms)
+    A = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)
+    bf = cfg.block_frames
+    tiles = bf // cfg.gate_frames
+    out = np.empty(bf * 2, np.float32)
+    preroll = args.preroll if args.preroll is not None else PREROLL[args.workload]
+
+    # Pre-roll to the workload's steady state (untimed).
+    t_pre = time.perf_counter()
+    for _ in range(preroll):
+        blk = drv.prepare(A.stats().active_voices)
+        H.feed(A, blk)
+        A.render(out)
+        drv.finish(A.stats().active_voices)
+    t_pre = time.perf_counter() - t_pre
+    B = A.clone()
+
+    # e2e: W + K blocks through the C ABI with host buffers; record inputs.
+    W, K = args.warmup, args.steps
+    rec, e2e_t, e2e_units, h2d, d2h = [], 0.0, 0, 0, 0
+    outs_a = []
+    for i in range(W + K):
+        live = A.stats().active_voices
+        blk = drv.prepare(live)
+        n_render = live + len(blk.cmds)
+        t0 = time.perf_counter()
+        H.feed(A, blk)
+        A.render(out)
+        t1 = time.perf_counter()
+        drv.finish(A.stats().active_voices)
+        rec.append((blk, n_render))
+        outs_a.append(out.copy())
+        if i >= W:
+            e2e_t += t1 - t0
+            e2e_units += n_render * bf
+            h2d += blk.gates.nbytes + blk.chan.nbytes + blk.cmds.nbytes
+            d2h += out.nbytes + 64
+
+    # value: replay the recorded blocks from HBM on the clone.
+    dev = []
+    for blk, n_render in rec:
+        g = torch.from_numpy(blk.gates.view(np.int32)).cuda()
+        c = torch.from_numpy(blk.chan.view(np.int32)).cuda()
+        cm = torch.from_numpy(blk.cmds.view(np.uint8).copy()).cuda() if len(blk.cmds) else None
+        o = torch.empty(bf * 2, dtype=torch.float32, device="cuda")
+        dev.append((blk, n_render, g, c, cm, o))
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(B.stream())
+
+    def enqueue(entry):
+        blk, n_render, g, c, cm, o = entry
+        for idx, data in blk.variants:
+            B.set_params_variant(idx, data)
+        B.enqueue_block_device(g.data_ptr(), c.data_ptr(), blk.bend, blk.gain, blk.variant,
+                               cm.data_ptr() if cm is not None else 0, len(blk.cmds), o.data_ptr())
+
+    for e in dev[:W]:
+        enqueue(e)
+    B.synchronize()
+    B.set_profile(True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for e in dev[W:]:
+        enqueue(e)
+    ev1.record(stream)
+    B.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dt_ms = ev0.elapsed_time(ev1)
+    passes, nblocks = B.timings_total()
+    units = sum(n for _, n, *_ in dev[W:]) * bf
+    # determinism: the replay must equal the host-buffer render byte for byte
+    same = all(np.array_equal(e[5].cpu().numpy(), outs_a[i]) for i, e in enumerate(dev))
+    launches = B.block_launches() * K
+
+    res = {
+        "units": units, "ms": dt_ms, "e2e_units": e2e_units, "e2e_s": e2e_t, "h2d": h2d // max(K, 1),
+        "d2h": d2h // max(K, 1), "render_ms": passes["render"] / max(nblocks, 1), "passes": passes,
+        "nblocks": nblocks, "mean_live": float(np.mean([n for _, n, *_ in dev[W:]])),
+        "same": same, "clocks": clk, "launches": launches, "preroll_s": t_pre, "preroll": preroll,
+        "tiles": tiles, "bf": bf, "max_voices": cfg.max_voices, "sample_rate": cfg.sample_rate,
+        "steal_percent": cfg.max_steal_percent, "stolen": B.stats().stolen, "dropped": B.stats().dropped,
+    }
+    B.close()
+    A.close()
+    return res
+
+
+# ---- the CPU restatement ---------------------------------------------------------------
+
+def run_oracle(workload, seed, threads, max_blocks, max_seconds):
+    """Time the CPU restatement of src/cpu.rs over the workload's first blocks."""
+    from kestrel_b200 import host as H
+    from oracle.binding import OracleSynth
+    cfg, bs, ms = H.config_workload(workload, seed=seed)
+    bank = H.Bank(bs, cfg)
+    drv = H.Driver(cfg, bank, ms)
+    orc = OracleSynth(cfg, bank.pool, bank.params, threads=threads)
+    out = np.empty(cfg.block_frames * 2, np.float32)
+    t_sum, units, blocks, live_max = 0.0, 0, 0, 0
+    per_block = []
+    while blocks < max_blocks and t_sum < max_seconds:
+        live = orc.stats().active_voices
+        blk = drv.prepare(live)
+        n_render = live + len(blk.cmds)
+        t0 = time.perf_counter()
+        H.feed(orc, blk)
+        orc.render(out, keep_mix64=False)
+        dt = time.perf_counter() - t0
+        drv.finish(orc.stats().active_voices)
+        t_sum += dt
+        units += n_render * cfg.block_frames
+        blocks += 1
+        live_max = max(live_max, n_render)
+        per_block.append((n_render, dt))
+    orc.close()
+    return {"value": units / t_sum if t_sum > 0 else 0.0, "blocks": blocks, "seconds": t_sum, "units": units,
+            "live_max": live_max, "per_block": per_block, "block_frames": cfg.block_frames,
+            "sample_rate": cfg.sample_rate}
+
+
+def workload_desc(name):
+    return {
+        "steal": "steal-saturation: 200M notes / 120 s, log-normal durations (median 6 s, sigma 0.5), "
+                 "1 preset x 128 zones, max_voices 8,388,608, steal-percent 10",
+        "black": "black-midi: 20M notes / 180 s, 60% in 1 ms clusters of 1k-50k, 128 presets, "
+                 "bend+CC7+CC11 every 10 ms, max_voices 1,048,576",
+        "plain": "plain: 100k notes / 30 s, 1 preset, max_voices 65,536",
+    }[name]
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    world, rank, local = dist_env()
+    metric = "voice-samples/s (x-realtime beside) at 1M-8M voices"
+    unit = "voice-samples/s"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        r = run_oracle(args.workload, args.seed, threads, args.warmup + args.steps, float("inf"))
+        # the first W blocks are warm-up
+        timed = r["per_block"][args.warmup:]
+        secs = sum(dt for _, dt in timed)
+        units = sum(n for n, _ in timed) * r["block_frames"]
+        value = units / secs if secs > 0 else 0.0
+        line = {
+            "metric": metric, "value": value, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(len(timed), 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "x_realtime": (len(timed) * r["block_frames"] / r["sample_rate"]) / secs if secs > 0 else 0.0,
+            "config": {"workload": workload_desc(args.workload), "steps_are": "the workload's first blocks",
+                       "live_voices_max": r["live_max"]},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                             "sample": f"blocks {args.warmup}..{args.warmup + len(timed) - 1} of the workload "
+                                       f"(up to {r['live_max']} voices), C++ restatement of src/cpu.rs, "
+                                       f"voice loop split over {threads} threads"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    r = run_cuda(args, world, rank, local)
+
+    units, ms_t, e2e_units, e2e_s = r["units"], r["ms"], r["e2e_units"], r["e2e_s"]
+    if world > 1:
+        import torch
+        t = torch.tensor([float(units), float(e2e_units)], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t)
+        m = torch.tensor([ms_t, e2e_s], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(m, op=torch.distributed.ReduceOp.MAX)
+        units, e2e_units = float(t[0]), float(t[1])
+        ms_t, e2e_s = float(m[0]), float(m[1])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        c = run_oracle(args.workload, args.seed, 1, 1 << 30, args.cpu_seconds)
+        cpu = {"value": c["value"], "unit": unit, "cores": 1, "kind": "port",
+               "sample": f"first {c['blocks']} blocks of the workload (up to {c['live_max']} voices, "
+                         f"{c['seconds']:.1f} s of CPU), C++ restatement of src/cpu.rs, one thread"}
+
+    if rank == 0:
+        K = args.steps
+        peak, peak_kind = measured_peaks()
+        n_render_mean = r["mean_live"]
+        bytes_launch = render_algorithmic_bytes(int(round(n_render_mean)), r["bf"], r["tiles"])
+        achieved = bytes_launch / (r["render_ms"] * 1e-3) / 1e9 if r["render_ms"] > 0 else 0.0
+        tpu = render_traffic_per_unit()
+        value = units / (ms_t * 1e-3)
+        line = {
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms_t / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "x_realtime": (K * r["bf"] / r["sample_rate"]) / (ms_t * 1e-3),
+            "config": {"workload": workload_desc(args.workload), "block_frames": r["bf"],
+                       "sample_rate": r["sample_rate"], "max_voices": r["max_voices"],
+                       "mean_voices_rendered": round(n_render_mean), "preroll_blocks": r["preroll"],
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (voice pool >= 1.8 GB at 8.4M voices)"
+                             if args.workload == "steal" else "inputs smaller than L2 between blocks",
+                       "replay_equals_host_render": r["same"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_render",
+                         "algorithmic_bytes_per_launch": bytes_launch,
+                         "launch_ms": r["render_ms"],
+                         "traffic": (tpu * n_render_mean * r["bf"]) if tpu else None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_units / e2e_s if e2e_s > 0 else 0.0, "unit": unit,
+                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+            "clocks": r["clocks"],
+            "gpu_launches": r["launches"],
+            "passes_ms_per_block": {k: v / max(r["nblocks"], 1) for k, v in r["passes"].items()},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -161,6 +161,12 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
                     uint32_t n_regions, uint32_t max_sample_len, kc_synth** out);
 void kc_synth_destroy(kc_synth* s);
 
+/* A second context on the same device in the same state: bank, params
+ * variants, voice pool and counters are copied device to device. No
+ * counterpart in the reference trait; it is how a render is checkpointed or
+ * forked (the benchmark forks one to replay recorded blocks from HBM). */
+int kc_synth_clone(kc_synth* src, kc_synth** out);
+
 /* Backend::set_gates (src/backend.rs:23-25): tiles * KC_GATE_SLOTS words,
  * tile-major; tiles = block_frames / gate_frames. */
 int kc_set_gates(kc_synth* s, const uint32_t* rows, size_t n);
@@ -192,6 +198,10 @@ const char* kc_name(const kc_synth* s);
  * the last render when timing is enabled (kc_set_profile). */
 int kc_set_profile(kc_synth* s, int on);
 int kc_timings(kc_synth* s, const char** names, double* ms, size_t cap, size_t* n);
+/* The same passes summed over every block completed since profiling was
+ * switched on (blocks enqueued back to back included), and the block count.
+ * No counterpart in the reference trait. */
+int kc_timings_total(kc_synth* s, double* ms, size_t cap, uint64_t* blocks);
 
 /* Message of the last failing call on this thread ("" when none). */
 const char* kc_last_error(void);

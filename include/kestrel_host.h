@@ -1,0 +1,190 @@
+/*
+ * kestrel_host.h -- C ABI of the host side that feeds the backend.
+ *
+ * Kestrel's driver (src/driver.rs) is the *caller* of the Backend trait: it
+ * owns the bank, the MIDI timeline, the note-off gate table, the channel
+ * controller table and admission, and hands the backend one block of inputs
+ * at a time. It is branchy table work that the reference keeps on the CPU by
+ * design (src/bank.rs:1-6), and so does this library. It is a C++17
+ * restatement of:
+ *
+ *   src/bank.rs     Region/RegionParams, build_voice, make_params, the
+ *                   admission preview tables, params variants
+ *   src/sf2.rs      generator flattening (build_region) and build_pool
+ *   src/resample.rs the load-time 32-tap x 512-phase Blackman sinc
+ *   src/voice.rs    GateTable, ChannelTable, admit_key/mix48/rank_gain_q
+ *   src/midi.rs     TempoClock
+ *   src/driver.rs   next_block: events, admission (strata ranking),
+ *                   materialise, controllers, LFO modulation
+ *   src/testkit.rs  the synthetic waveforms the seeded banks are built from
+ *
+ * A soundfont here is described by generator lists in memory (the same
+ * (operator, amount) pairs an SF2 pgen/igen chunk holds) rather than parsed
+ * from a RIFF file; MIDI is a seeded synthetic event stream with the shapes
+ * of the benchmark configurations. The block inputs it produces are the
+ * backend's arguments verbatim: kc_spawn_cmd records, gate rows, channel rows.
+ */
+#ifndef KESTREL_HOST_H
+#define KESTREL_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kestrel_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Config fields the host side reads beyond kc_config (src/config.rs). */
+typedef struct kh_options {
+    float master_volume;            /* 1.0 */
+    uint32_t filter_enabled;        /* 1 */
+    uint32_t max_layers;            /* 16 */
+    uint32_t default_channel_volume;/* 127 */
+    uint32_t resample_pool;         /* 1: rebuild the pool at the output rate */
+    uint64_t sample_pool_budget;    /* bytes, 2 GiB */
+} kh_options;
+
+void kh_options_default(kh_options* o);
+
+/* ---- synthetic soundfonts ------------------------------------------------ */
+
+/* The seeded synthetic banks of the benchmark configurations: `presets`
+ * presets, each one instrument of 128 zones (zone k plays key k from sample k,
+ * root k). Sample k is `sample_frames` frames at `sample_rate` Hz: a sine at
+ * the key's pitch plus white noise, looped over its last `loop_frames` frames.
+ * Preset 0 uses the base envelope/filter generators below; with
+ * `random_generators` every preset draws its own (seeded). */
+typedef struct kh_synth_bank_spec {
+    uint32_t presets;            /* 1 or 128 */
+    uint32_t sample_frames;      /* 32768 */
+    uint32_t sample_rate;        /* 44100 */
+    uint32_t loop_frames;        /* 8192 */
+    float amplitude;             /* 0.5 */
+    float noise;                 /* 0.01 (1% white noise) */
+    int16_t attack_tc;           /* -9172: 5 ms */
+    int16_t decay_tc;            /* -2786: 200 ms */
+    int16_t sustain_cb;          /* 60: -6 dB */
+    int16_t release_tc;          /* -2084: 300 ms */
+    int16_t filter_fc_cents;     /* 11913: 8 kHz */
+    int16_t filter_q_cb;         /* 30: Q 1 */
+    uint32_t random_generators;  /* 0/1 */
+    uint64_t seed;
+} kh_synth_bank_spec;
+
+void kh_synth_bank_spec_default(kh_synth_bank_spec* s);
+
+typedef struct kh_bank kh_bank;
+
+kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg,
+                           const kh_options* opt);
+void kh_bank_destroy(kh_bank* b);
+/* Views into the bank; valid until kh_bank_destroy. */
+int kh_bank_pool(const kh_bank* b, const int16_t** pool, uint64_t* len);
+int kh_bank_params(const kh_bank* b, const kc_region_params** params, uint32_t* len);
+uint32_t kh_bank_regions(const kh_bank* b);
+uint32_t kh_bank_presets(const kh_bank* b);
+uint32_t kh_bank_max_sample_len(const kh_bank* b);
+uint32_t kh_bank_pool_rate(const kh_bank* b);
+
+/* ---- synthetic MIDI ------------------------------------------------------ */
+
+/* A seeded event stream with the shapes of the benchmark configurations:
+ * Poisson onsets (optionally a share packed into 1 ms clusters), uniform keys
+ * and velocities, log-normal durations, optional pitch-bend/CC7/CC11 curves
+ * every `cc_period_ms` per channel and program changes every
+ * `program_period_s` per channel. Events are produced lazily in tick order, so
+ * a 200M-note stream never sits in memory. */
+typedef struct kh_midi_spec {
+    uint64_t notes;
+    double seconds;
+    uint32_t channels;           /* 16 */
+    uint32_t key_lo, key_hi;     /* 21, 108 */
+    uint32_t vel_lo, vel_hi;     /* 1, 127 */
+    double dur_median_s;         /* 0.150 */
+    double dur_sigma;            /* 1.0 */
+    double cluster_share;        /* 0: no clusters; 0.6 for the black-MIDI config */
+    uint32_t cluster_lo, cluster_hi; /* notes per 1 ms cluster */
+    double cc_period_ms;         /* 0: no controller curves; 10 for config 2 */
+    double program_period_s;     /* 0: every channel stays on program 0 */
+    uint32_t programs;           /* presets to spread program changes over */
+    uint32_t ppq;                /* ticks per quarter note, 9600 */
+    uint64_t seed;
+} kh_midi_spec;
+
+void kh_midi_spec_default(kh_midi_spec* s);
+
+/* ---- the driver ---------------------------------------------------------- */
+
+typedef struct kh_driver kh_driver;
+
+/* One block of backend inputs, produced by kh_driver_prepare. The pointers
+ * stay valid until the next prepare call. */
+typedef struct kh_block {
+    const uint32_t* gates;        /* tiles * 2048 */
+    size_t n_gates;
+    const uint32_t* chan;         /* tiles * 64 */
+    size_t n_chan;
+    int bend, gain, variant;      /* set_channels flags */
+    const kc_spawn_cmd* cmds;     /* admitted and materialised, candidate order */
+    size_t n_cmds;
+    uint32_t n_variants;          /* params variants to install first (kh_driver_variant) */
+    uint32_t live;                /* voices alive when admission ran */
+    uint32_t want;                /* candidates queued */
+    uint32_t take;                /* candidates admitted */
+    uint64_t block_index;
+    uint64_t notes;               /* note-ons handled so far */
+} kh_block;
+
+kh_driver* kh_driver_open(const kc_config* cfg, const kh_options* opt, const kh_bank* bank,
+                          const kh_midi_spec* midi);
+void kh_driver_destroy(kh_driver* d);
+
+/* Driver::next_block (src/driver.rs:434-594) up to the backend's spawn:
+ * drains this block's events, publishes gate and channel rows, runs admission
+ * against `live` (the backend's active_voices, as the reference reads
+ * backend.stats() at src/driver.rs:557), and materialises the admitted
+ * voices. */
+int kh_driver_prepare(kh_driver* d, uint32_t live, kh_block* out);
+/* The i-th params variant to install before this block's spawn. */
+int kh_driver_variant(kh_driver* d, uint32_t i, uint32_t* index, const kc_region_params** data,
+                      size_t* n);
+/* The rest of next_block after render (src/driver.rs:619-642): returns
+ * *more = 0 once the file and its tail are done. */
+int kh_driver_finish(kh_driver* d, uint64_t active_voices, int* more);
+
+const char* kh_last_error(void);
+
+/* ---- the pieces the reference's own unit tests exercise ------------------ *
+ * The gate table (src/voice.rs:212-452) on its own, and the bank's DSP
+ * helpers, so the reference's in-module tests (src/voice.rs:660-766,
+ * src/bank.rs:981-1035, src/resample.rs:109-171) can be restated against
+ * this build. */
+typedef struct kh_gates kh_gates;
+kh_gates* kh_gates_new(uint32_t block_frames, uint32_t gate_frames);
+void kh_gates_destroy(kh_gates* g);
+void kh_gates_begin_block(kh_gates* g);
+void kh_gates_end_block(kh_gates* g);
+uint32_t kh_gates_note_on(kh_gates* g, uint8_t ch, uint8_t key, uint32_t frame);
+void kh_gates_note_off(kh_gates* g, uint8_t ch, uint8_t key, uint32_t frame);
+void kh_gates_set_sustain(kh_gates* g, uint8_t ch, int down, uint32_t frame);
+void kh_gates_set_sostenuto(kh_gates* g, uint8_t ch, int down, uint32_t frame);
+uint32_t kh_gates_row(const kh_gates* g, uint32_t tile, uint32_t slot);
+uint32_t kh_gates_tiles(const kh_gates* g);
+uint64_t kh_gates_sounding(const kh_gates* g);
+
+float kh_velocity_atten_cb(uint8_t vel, float veltrack);
+void kh_biquad_lowpass(float fc, float q_cb, float sr, float* b0, float* b1, float* a1, float* a2);
+float kh_timecents_to_secs(float tc);
+/* resample::resample_i16; `out` holds at least round(n * ratio) + 1 samples.
+ * Returns the output length. */
+size_t kh_resample_i16(const int16_t* src, size_t n, double ratio, int16_t* out, size_t cap);
+uint64_t kh_mix48(uint64_t index);
+uint64_t kh_rank_gain_q(float gain_l, float gain_r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KESTREL_HOST_H */

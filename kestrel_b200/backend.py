@@ -45,6 +45,19 @@ class CudaSynth:
         self.tiles = cfg.block_frames // cfg.gate_frames
         self.params_per = params.size
 
+    def clone(self) -> "CudaSynth":
+        """A second context in this one's exact state (kc_synth_clone)."""
+        h = C.c_void_p()
+        N.check(self._lib.kc_synth_clone(self._h, C.byref(h)), self._lib)
+        other = object.__new__(CudaSynth)
+        other._lib = self._lib
+        other.cfg = self.cfg
+        other._h = h
+        other.block_frames = self.block_frames
+        other.tiles = self.tiles
+        other.params_per = self.params_per
+        return other
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.kc_synth_destroy(self._h)
@@ -100,6 +113,14 @@ class CudaSynth:
         n = C.c_size_t()
         N.check(self._lib.kc_timings(self._h, names, ms, 8, C.byref(n)), self._lib)
         return [(names[i].decode(), ms[i]) for i in range(n.value)]
+
+    def timings_total(self) -> tuple[dict, int]:
+        """Per-pass milliseconds summed over all profiled blocks, and their count."""
+        ms = (C.c_double * 8)()
+        nb = C.c_uint64()
+        N.check(self._lib.kc_timings_total(self._h, ms, 8, C.byref(nb)), self._lib)
+        names = ["steal", "spawn", "render", "reduce", "compact"]
+        return {k: ms[i] for i, k in enumerate(names)}, nb.value
 
     # ---- device-resident form and inspection --------------------------------
     def enqueue_block_device(self, d_gates: int, d_chan: int, bend: bool, gain: bool, variant: bool,

@@ -1,0 +1,94 @@
+// midi.h -- events, the tempo clock (src/midi.rs:17-34, 376-431), and the
+// seeded synthetic event stream that stands in for a black-MIDI file.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <queue>
+#include <random>
+#include <vector>
+
+#include "../../../include/kestrel_host.h"
+
+namespace kh {
+
+// midi::Event (src/midi.rs:17-29).
+enum class EvType : uint8_t { NoteOn, NoteOff, Cc, Program, PitchBend, Tempo, Other };
+
+struct Event {
+    EvType type = EvType::Other;
+    uint8_t ch = 0, a = 0, b = 0;  // NoteOn: key, vel; NoteOff: key; Cc: num, val; Program: val
+    int16_t bend = 0;              // PitchBend value, -8192..8191
+    uint32_t tempo = 0;            // microseconds per quarter note
+};
+
+// TempoClock (src/midi.rs:378-431), PPQ division only.
+struct TempoClock {
+    double sample_rate = 48000.0;
+    uint32_t ppq = 960;
+    uint64_t base_tick = 0;
+    double base_frame = 0.0;
+    double frames_per_tick = 0.0;
+
+    TempoClock() = default;
+    TempoClock(uint32_t ppq_, uint32_t rate) : sample_rate((double)rate), ppq(ppq_) { set_tempo_raw(500000); }
+    void set_tempo_raw(uint32_t us_per_qn) {
+        const double p = (double)std::max<uint32_t>(ppq, 1);
+        frames_per_tick = ((double)us_per_qn * 1e-6) * sample_rate / p;
+    }
+    void set_tempo(uint64_t tick, uint32_t us_per_qn) {
+        base_frame = frame_at(tick);
+        base_tick = tick;
+        set_tempo_raw(us_per_qn);
+    }
+    double frame_at(uint64_t tick) const { return base_frame + (double)(tick - base_tick) * frames_per_tick; }
+};
+
+// The synthetic stream. Onsets are generated one window of time at a time:
+// background notes as a Poisson process, plus (optionally) 1 ms clusters of
+// many simultaneous notes; every onset schedules its note-off in a min-heap.
+// Controller curves and program changes run on their own schedule. The three
+// sources are merged by tick (at equal ticks: offs, then controllers, then
+// ons), so the stream is a pure function of the spec.
+class SynthMidi {
+   public:
+    explicit SynthMidi(const kh_midi_spec& s);
+    // Next event in tick order; false when the stream is exhausted.
+    bool next(uint64_t* tick, Event* ev);
+    uint32_t ppq() const { return spec_.ppq; }
+
+   private:
+    struct Off {
+        uint64_t tick, seq;
+        uint8_t ch, key;
+        bool operator>(const Off& o) const { return tick != o.tick ? tick > o.tick : seq > o.seq; }
+    };
+    struct On {
+        uint64_t tick;
+        uint8_t ch, key, vel;
+        double dur_s;
+    };
+    void refill_onsets();
+    bool next_ctrl(uint64_t* tick, Event* ev, bool peek_only);
+    uint64_t tick_of(double t) const { return (uint64_t)std::llround(t * ticks_per_s_); }
+
+    kh_midi_spec spec_;
+    std::mt19937_64 rng_;
+    double ticks_per_s_;
+    double window_t_ = 0.0;             // onsets generated up to here
+    uint64_t onsets_made_ = 0;
+    std::vector<On> ons_;
+    size_t on_pos_ = 0;
+    std::priority_queue<Off, std::vector<Off>, std::greater<Off>> offs_;
+    uint64_t off_seq_ = 0;
+    // controller schedule
+    uint64_t ctrl_step_ = 0;            // index of the next controller time step
+    uint32_t ctrl_sub_ = 0;             // which event within the step
+    std::vector<Event> ctrl_buf_;
+    uint64_t ctrl_tick_ = 0;
+    bool ctrl_done_ = false;
+    std::vector<double> phase_;         // per-channel curve phases
+};
+
+}  // namespace kh

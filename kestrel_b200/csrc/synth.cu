@@ -102,6 +102,7 @@ struct kc_synth {
     uint32_t params_per = 0;    // entries per params variant
     uint32_t n_slots = 0;       // params variant slots
     uint64_t pcm_len = 0;
+    uint32_t n_regions = 0, max_sample_len = 0;
     SortLayout sort{};
 
     // device buffers
@@ -148,6 +149,12 @@ struct kc_synth {
     cudaEvent_t ev[N_TIMERS + 1] = {};
     double last_ms[N_TIMERS] = {};
     bool have_timings = false;
+    // Profiling over many blocks in flight: one event set per enqueued block,
+    // read back at the next synchronisation.
+    std::vector<std::vector<cudaEvent_t>> ring;
+    size_t ring_pending = 0;
+    double total_ms[N_TIMERS] = {};
+    uint64_t total_blocks = 0;
 };
 
 namespace {
@@ -180,6 +187,8 @@ void free_all(kc_synth* s) {
     cudaFreeHost(s->h_st);
     for (auto& e : s->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& set : s->ring)
+        for (auto& e : set) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -225,7 +234,16 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     pa.steal_span = std::max<uint32_t>(span, 1);
     pa.render_warps = s->render_warps;
 
-    if (s->profile) cudaEventRecord(s->ev[0], q);
+    cudaEvent_t* ev = s->ev;
+    if (s->profile) {
+        if (s->ring_pending == s->ring.size()) {
+            std::vector<cudaEvent_t> set(N_TIMERS + 1);
+            for (auto& e : set) KC_CUDA(cudaEventCreate(&e));
+            s->ring.push_back(std::move(set));
+        }
+        ev = s->ring[s->ring_pending++].data();
+    }
+    if (s->profile) cudaEventRecord(ev[0], q);
     k_admit<<<1, 256, 0, q>>>(pa, s->sel_hist, s->ctl, n_cmds, chan_active);
     // ---- 1. steal ----
     if (c.steal_rule != KC_STEAL_DROP_NEW) {
@@ -235,10 +253,10 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
         }
         k_mark_stolen<<<s->pool_ctas, 256, 0, q>>>(pa);
     }
-    if (s->profile) cudaEventRecord(s->ev[1], q);
+    if (s->profile) cudaEventRecord(ev[1], q);
     // ---- 2. spawn ----
     k_spawn<<<s->pool_ctas, 256, 0, q>>>(pa, d_cmds);
-    if (s->profile) cudaEventRecord(s->ev[2], q);
+    if (s->profile) cudaEventRecord(ev[2], q);
     // ---- 3. render ----
     RenderArgs ra{};
     ra.pool = pa.pool;
@@ -263,14 +281,14 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode);
     void* args[] = {&ra};
     KC_CUDA(cudaLaunchKernel(fn, dim3(s->render_ctas), dim3(RENDER_WARPS * 32), args, s->render_smem, q));
-    if (s->profile) cudaEventRecord(s->ev[3], q);
+    if (s->profile) cudaEventRecord(ev[3], q);
     // ---- 4. reduce ----
     const uint32_t samples = c.block_frames * 2;
     if (c.mix_mode == KC_MIX_F32_TREE)
         k_reduce<0><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
     else
         k_reduce<1><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
-    if (s->profile) cudaEventRecord(s->ev[4], q);
+    if (s->profile) cudaEventRecord(ev[4], q);
     // ---- 5. compact (and sort) ----
     k_compact_count<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
     k_scan_counts<<<1, 1024, 0, q>>>(s->counts, s->compact_ctas, s->total);
@@ -293,10 +311,26 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
         }
         k_sort_gather<<<s->pool_ctas, 256, 0, q>>>(pa, s->idx[cur]);
     }
-    if (s->profile) cudaEventRecord(s->ev[5], q);
+    if (s->profile) cudaEventRecord(ev[5], q);
     KC_CUDA(cudaGetLastError());
     s->parity ^= 1;
     return KC_OK;
+}
+
+// After a synchronisation: fold every profiled block's pass times into the
+// totals and keep the last block's as `last_ms`.
+void drain_timings(kc_synth* s) {
+    for (size_t b = 0; b < s->ring_pending; ++b) {
+        for (int i = 0; i < N_TIMERS; ++i) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ring[b][i], s->ring[b][i + 1]);
+            s->total_ms[i] += ms;
+            s->last_ms[i] = ms;
+        }
+        s->total_blocks += 1;
+        s->have_timings = true;
+    }
+    s->ring_pending = 0;
 }
 
 uint32_t launches_per_block(const kc_synth* s) {
@@ -380,6 +414,8 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     s->n_slots = cfg->max_param_variants;
     s->pcm_len = pool_len;
     s->sort = plan_sort(n_regions, max_sample_len);
+    s->n_regions = n_regions;
+    s->max_sample_len = max_sample_len;
 
     // Launch geometry: the render grid is every resident CTA of the device,
     // and the partial buffer has one slice per render warp.
@@ -402,13 +438,13 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMalloc(&s->pool[0], pool_words * 4));
     KC_TRY(cudaMalloc(&s->pool[1], pool_words * 4));
     KC_TRY(cudaMalloc(&s->pcm, std::max<uint64_t>(pool_len, 1) * 2 + 64));
-    if (pool_len) KC_TRY(cudaMemcpy(s->pcm, pool, pool_len * 2, cudaMemcpyHostToDevice));
+    if (pool_len) KC_TRY(cudaMemcpy(s->pcm, pool, pool_len * 2, cudaMemcpyDefault));
     const size_t per_bytes = (size_t)params_len * sizeof(kc_region_params);
     KC_TRY(cudaMalloc(&s->params, per_bytes * s->n_slots));
     // Every slot starts as a copy of the bank's table, which is what
     // CpuSynth::params_of falls back to for a variant never uploaded.
     for (uint32_t v = 0; v < s->n_slots; ++v)
-        KC_TRY(cudaMemcpy((char*)s->params + v * per_bytes, params, per_bytes, cudaMemcpyHostToDevice));
+        KC_TRY(cudaMemcpy((char*)s->params + v * per_bytes, params, per_bytes, cudaMemcpyDefault));
     const size_t gate_words = (size_t)s->tiles * KC_GATE_SLOTS;
     const size_t chan_words = (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS;
     KC_TRY(cudaMalloc(&s->gates, gate_words * 4));
@@ -444,6 +480,34 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     for (auto& e : s->ev) KC_TRY(cudaEventCreate(&e));
     KC_TRY(cudaDeviceSynchronize());
 #undef KC_TRY
+    *out = s;
+    return KC_OK;
+}
+
+int kc_synth_clone(kc_synth* src, kc_synth** out) {
+    if (!src || !out) return fail(KC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    cudaSetDevice(src->device);
+    KC_CUDA(cudaStreamSynchronize(src->stream));
+    kc_synth* s = nullptr;
+    // The bank and variant-0 table come straight from the source's device
+    // copies (cudaMemcpyDefault resolves device pointers under UVA).
+    if (int rc = kc_synth_create(&src->cfg, src->pcm, src->pcm_len, src->params, src->params_per,
+                                 src->n_regions, src->max_sample_len, &s))
+        return rc;
+    auto bail = [&](cudaError_t e) {
+        kc_synth_destroy(s);
+        return fail(KC_ERR_CUDA, std::string("clone: ") + cudaGetErrorString(e));
+    };
+    const size_t per_bytes = (size_t)src->params_per * sizeof(kc_region_params);
+    cudaError_t e = cudaMemcpy(s->params, src->params, per_bytes * src->n_slots, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(s->pool[0], src->pool[src->parity], (size_t)VOICE_FIELDS * src->cap * 4,
+                       cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->st, src->st, sizeof(DevState), cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) return bail(e);
+    s->parity = 0;
+    s->stats = src->stats;
     *out = s;
     return KC_OK;
 }
@@ -551,14 +615,7 @@ int kc_render(kc_synth* s, float* out, size_t n) {
     s->stats.dropped = s->h_st->dropped;
     uint32_t pb = s->h_st->peak_bits;
     std::memcpy(&s->stats.peak, &pb, 4);
-    if (s->profile) {
-        for (int i = 0; i < N_TIMERS; ++i) {
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, s->ev[i], s->ev[i + 1]);
-            s->last_ms[i] = ms;
-        }
-        s->have_timings = true;
-    }
+    drain_timings(s);
     if (s->h_st->error)
         return fail(KC_ERR_DEVICE, "device error word " + std::to_string(s->h_st->error));
     return KC_OK;
@@ -574,8 +631,20 @@ const char* kc_name(const kc_synth*) { return "cuda-sm100a"; }
 
 int kc_set_profile(kc_synth* s, int on) {
     if (!s) return fail(KC_ERR_INVALID, "null synth");
+    cudaSetDevice(s->device);
+    KC_CUDA(cudaStreamSynchronize(s->stream));
+    drain_timings(s);
     s->profile = on != 0;
     s->have_timings = false;
+    for (auto& t : s->total_ms) t = 0.0;
+    s->total_blocks = 0;
+    return KC_OK;
+}
+
+int kc_timings_total(kc_synth* s, double* ms, size_t cap, uint64_t* blocks) {
+    if (!s || !blocks) return fail(KC_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < std::min<size_t>(cap, N_TIMERS); ++i) ms[i] = s->total_ms[i];
+    *blocks = s->total_blocks;
     return KC_OK;
 }
 
@@ -604,6 +673,7 @@ int kc_synchronize(kc_synth* s) {
     cudaSetDevice(s->device);
     KC_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
     KC_CUDA(cudaStreamSynchronize(s->stream));
+    drain_timings(s);
     s->stats.active_voices = s->h_st->live;
     s->stats.stolen = s->h_st->stolen;
     s->stats.dropped = s->h_st->dropped;

@@ -1,0 +1,347 @@
+"""The host side that feeds a backend: synthetic banks, MIDI and the driver.
+
+Binds libkestrel_host.so (include/kestrel_host.h), the C++ restatement of
+Kestrel's driver (src/driver.rs), bank (src/bank.rs) and SF2 flattening
+(src/sf2.rs). ``run_blocks`` is Driver::next_block's loop
+(src/bin/kestrel.rs:311-365 calls it once per block): prepare the block's
+inputs, hand them to a backend in the reference's call order, render.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from . import native as N
+
+HOST_LIB_PATH = Path(__file__).resolve().parent / "libkestrel_host.so"
+
+
+class KhOptions(C.Structure):
+    _fields_ = [("master_volume", C.c_float), ("filter_enabled", C.c_uint32), ("max_layers", C.c_uint32),
+                ("default_channel_volume", C.c_uint32), ("resample_pool", C.c_uint32),
+                ("sample_pool_budget", C.c_uint64)]
+
+
+class KhSynthBankSpec(C.Structure):
+    _fields_ = [("presets", C.c_uint32), ("sample_frames", C.c_uint32), ("sample_rate", C.c_uint32),
+                ("loop_frames", C.c_uint32), ("amplitude", C.c_float), ("noise", C.c_float),
+                ("attack_tc", C.c_int16), ("decay_tc", C.c_int16), ("sustain_cb", C.c_int16),
+                ("release_tc", C.c_int16), ("filter_fc_cents", C.c_int16), ("filter_q_cb", C.c_int16),
+                ("random_generators", C.c_uint32), ("seed", C.c_uint64)]
+
+
+class KhMidiSpec(C.Structure):
+    _fields_ = [("notes", C.c_uint64), ("seconds", C.c_double), ("channels", C.c_uint32),
+                ("key_lo", C.c_uint32), ("key_hi", C.c_uint32), ("vel_lo", C.c_uint32), ("vel_hi", C.c_uint32),
+                ("dur_median_s", C.c_double), ("dur_sigma", C.c_double), ("cluster_share", C.c_double),
+                ("cluster_lo", C.c_uint32), ("cluster_hi", C.c_uint32), ("cc_period_ms", C.c_double),
+                ("program_period_s", C.c_double), ("programs", C.c_uint32), ("ppq", C.c_uint32),
+                ("seed", C.c_uint64)]
+
+
+class KhBlock(C.Structure):
+    _fields_ = [("gates", C.POINTER(C.c_uint32)), ("n_gates", C.c_size_t), ("chan", C.POINTER(C.c_uint32)),
+                ("n_chan", C.c_size_t), ("bend", C.c_int), ("gain", C.c_int), ("variant", C.c_int),
+                ("cmds", C.c_void_p), ("n_cmds", C.c_size_t), ("n_variants", C.c_uint32), ("live", C.c_uint32),
+                ("want", C.c_uint32), ("take", C.c_uint32), ("block_index", C.c_uint64), ("notes", C.c_uint64)]
+
+
+_P = C.c_void_p
+HOST_SYMBOLS = {
+    "kh_options_default": (None, [C.POINTER(KhOptions)]),
+    "kh_synth_bank_spec_default": (None, [C.POINTER(KhSynthBankSpec)]),
+    "kh_bank_synthetic": (_P, [C.POINTER(KhSynthBankSpec), C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
+    "kh_bank_destroy": (None, [_P]),
+    "kh_bank_pool": (C.c_int, [_P, C.POINTER(C.POINTER(C.c_int16)), C.POINTER(C.c_uint64)]),
+    "kh_bank_params": (C.c_int, [_P, C.POINTER(_P), C.POINTER(C.c_uint32)]),
+    "kh_bank_regions": (C.c_uint32, [_P]),
+    "kh_bank_presets": (C.c_uint32, [_P]),
+    "kh_bank_max_sample_len": (C.c_uint32, [_P]),
+    "kh_bank_pool_rate": (C.c_uint32, [_P]),
+    "kh_midi_spec_default": (None, [C.POINTER(KhMidiSpec)]),
+    "kh_driver_open": (_P, [C.POINTER(N.KcConfig), C.POINTER(KhOptions), _P, C.POINTER(KhMidiSpec)]),
+    "kh_driver_destroy": (None, [_P]),
+    "kh_driver_prepare": (C.c_int, [_P, C.c_uint32, C.POINTER(KhBlock)]),
+    "kh_driver_variant": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    "kh_driver_finish": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
+    "kh_last_error": (C.c_char_p, []),
+    "kh_gates_new": (_P, [C.c_uint32, C.c_uint32]),
+    "kh_gates_destroy": (None, [_P]),
+    "kh_gates_begin_block": (None, [_P]),
+    "kh_gates_end_block": (None, [_P]),
+    "kh_gates_note_on": (C.c_uint32, [_P, C.c_uint8, C.c_uint8, C.c_uint32]),
+    "kh_gates_note_off": (None, [_P, C.c_uint8, C.c_uint8, C.c_uint32]),
+    "kh_gates_set_sustain": (None, [_P, C.c_uint8, C.c_int, C.c_uint32]),
+    "kh_gates_set_sostenuto": (None, [_P, C.c_uint8, C.c_int, C.c_uint32]),
+    "kh_gates_row": (C.c_uint32, [_P, C.c_uint32, C.c_uint32]),
+    "kh_gates_tiles": (C.c_uint32, [_P]),
+    "kh_gates_sounding": (C.c_uint64, [_P]),
+    "kh_velocity_atten_cb": (C.c_float, [C.c_uint8, C.c_float]),
+    "kh_biquad_lowpass": (None, [C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                 C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "kh_timecents_to_secs": (C.c_float, [C.c_float]),
+    "kh_resample_i16": (C.c_size_t, [_P, C.c_size_t, C.c_double, _P, C.c_size_t]),
+    "kh_mix48": (C.c_uint64, [C.c_uint64]),
+    "kh_rank_gain_q": (C.c_uint64, [C.c_float, C.c_float]),
+}
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not HOST_LIB_PATH.exists():
+            raise RuntimeError(f"{HOST_LIB_PATH} is not built; run `python -m kestrel_b200.build`")
+        _lib = N.bind(C.CDLL(str(HOST_LIB_PATH)), HOST_SYMBOLS)
+    return _lib
+
+
+class GateTable:
+    """voice::GateTable (src/voice.rs:212-452) from the host library."""
+
+    def __init__(self, block_frames: int, gate_frames: int):
+        self._lib = lib()
+        self._h = self._lib.kh_gates_new(block_frames, gate_frames)
+        if not self._h:
+            raise ValueError("gate_frames must divide block_frames")
+        self.tiles = self._lib.kh_gates_tiles(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.kh_gates_destroy(self._h)
+            self._h = None
+
+    @staticmethod
+    def slot(ch: int, key: int) -> int:
+        return (ch & 15) * 128 + (key & 127)
+
+    def begin_block(self):
+        self._lib.kh_gates_begin_block(self._h)
+
+    def end_block(self):
+        self._lib.kh_gates_end_block(self._h)
+
+    def note_on(self, ch, key, frame) -> int:
+        return self._lib.kh_gates_note_on(self._h, ch, key, frame)
+
+    def note_off(self, ch, key, frame):
+        self._lib.kh_gates_note_off(self._h, ch, key, frame)
+
+    def set_sustain(self, ch, down, frame):
+        self._lib.kh_gates_set_sustain(self._h, ch, int(down), frame)
+
+    def set_sostenuto(self, ch, down, frame):
+        self._lib.kh_gates_set_sostenuto(self._h, ch, int(down), frame)
+
+    def row(self, tile: int) -> np.ndarray:
+        return np.array([self._lib.kh_gates_row(self._h, tile, s) for s in range(2048)], np.uint32)
+
+    def sounding(self) -> int:
+        return self._lib.kh_gates_sounding(self._h)
+
+
+def velocity_atten_cb(vel: int, veltrack: float) -> float:
+    return lib().kh_velocity_atten_cb(vel, veltrack)
+
+
+def biquad_lowpass(fc: float, q_cb: float, sr: float):
+    o = [C.c_float() for _ in range(4)]
+    lib().kh_biquad_lowpass(fc, q_cb, sr, *[C.byref(x) for x in o])
+    return tuple(np.float32(x.value) for x in o)
+
+
+def timecents_to_secs(tc: float) -> float:
+    return lib().kh_timecents_to_secs(tc)
+
+
+def resample_i16(src: np.ndarray, ratio: float) -> np.ndarray:
+    src = np.ascontiguousarray(src, np.int16)
+    cap = int(round(src.size * ratio)) + 2
+    out = np.empty(cap, np.int16)
+    n = lib().kh_resample_i16(N.ptr(src), src.size, ratio, N.ptr(out), cap)
+    return out[:n].copy()
+
+
+def mix48(i: int) -> int:
+    return lib().kh_mix48(i)
+
+
+def rank_gain_q(gl: float, gr: float) -> int:
+    return lib().kh_rank_gain_q(gl, gr)
+
+
+def options(**kw) -> KhOptions:
+    o = KhOptions()
+    lib().kh_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def bank_spec(**kw) -> KhSynthBankSpec:
+    s = KhSynthBankSpec()
+    lib().kh_synth_bank_spec_default(C.byref(s))
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def midi_spec(**kw) -> KhMidiSpec:
+    s = KhMidiSpec()
+    lib().kh_midi_spec_default(C.byref(s))
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+class Bank:
+    """A loaded bank: the i16 sample pool and the variant-0 params table."""
+
+    def __init__(self, spec: KhSynthBankSpec, cfg: N.KcConfig, opt: KhOptions | None = None):
+        self._lib = lib()
+        self.opt = opt or options()
+        h = self._lib.kh_bank_synthetic(C.byref(spec), C.byref(cfg), C.byref(self.opt))
+        if not h:
+            raise RuntimeError(self._lib.kh_last_error().decode())
+        self._h = h
+        p = C.POINTER(C.c_int16)()
+        n = C.c_uint64()
+        self._lib.kh_bank_pool(h, C.byref(p), C.byref(n))
+        self.pool = np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0, np.int16)
+        pp = C.c_void_p()
+        m = C.c_uint32()
+        self._lib.kh_bank_params(h, C.byref(pp), C.byref(m))
+        self.params = np.frombuffer((C.c_char * (m.value * 48)).from_address(pp.value),
+                                    dtype=N.PARAMS_DTYPE).copy()
+        self.regions = self._lib.kh_bank_regions(h)
+        self.presets = self._lib.kh_bank_presets(h)
+        self.max_sample_len = self._lib.kh_bank_max_sample_len(h)
+        self.pool_rate = self._lib.kh_bank_pool_rate(h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.kh_bank_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+@dataclass
+class BlockInputs:
+    """One block's backend arguments, owned (copied out of the driver)."""
+    gates: np.ndarray
+    chan: np.ndarray
+    bend: bool
+    gain: bool
+    variant: bool
+    cmds: np.ndarray
+    variants: list = field(default_factory=list)
+    live: int = 0
+    want: int = 0
+    take: int = 0
+
+
+class Driver:
+    def __init__(self, cfg: N.KcConfig, bank: Bank, midi: KhMidiSpec):
+        self._lib = lib()
+        self.bank = bank
+        h = self._lib.kh_driver_open(C.byref(cfg), C.byref(bank.opt), bank._h, C.byref(midi))
+        if not h:
+            raise RuntimeError(self._lib.kh_last_error().decode())
+        self._h = h
+        self.more = True
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.kh_driver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def prepare(self, live: int) -> BlockInputs:
+        b = KhBlock()
+        self._lib.kh_driver_prepare(self._h, live, C.byref(b))
+        gates = np.ctypeslib.as_array(b.gates, shape=(b.n_gates,)).copy()
+        chan = np.ctypeslib.as_array(b.chan, shape=(b.n_chan,)).copy()
+        if b.n_cmds:
+            cmds = np.frombuffer((C.c_char * (b.n_cmds * 76)).from_address(b.cmds), dtype=N.SPAWN_DTYPE).copy()
+        else:
+            cmds = np.zeros(0, N.SPAWN_DTYPE)
+        variants = []
+        for i in range(b.n_variants):
+            idx = C.c_uint32()
+            data = C.c_void_p()
+            n = C.c_size_t()
+            self._lib.kh_driver_variant(self._h, i, C.byref(idx), C.byref(data), C.byref(n))
+            arr = np.frombuffer((C.c_char * (n.value * 48)).from_address(data.value), dtype=N.PARAMS_DTYPE).copy()
+            variants.append((idx.value, arr))
+        return BlockInputs(gates, chan, bool(b.bend), bool(b.gain), bool(b.variant), cmds, variants, b.live, b.want,
+                           b.take)
+
+    def finish(self, active_voices: int) -> bool:
+        more = C.c_int()
+        self._lib.kh_driver_finish(self._h, active_voices, C.byref(more))
+        self.more = bool(more.value)
+        return self.more
+
+
+def feed(backend, blk: BlockInputs) -> None:
+    """Hand one block to a backend in Driver::next_block's order
+    (src/driver.rs:531-588): variants, gates, channels, spawn."""
+    for idx, data in blk.variants:
+        backend.set_params_variant(idx, data)
+    backend.set_gates(blk.gates)
+    backend.set_channels(blk.chan, blk.bend, blk.gain, blk.variant)
+    backend.spawn(blk.cmds)
+
+
+def run_blocks(backend, driver: Driver, n_blocks: int, record: bool = False, on_block=None):
+    """Drive `backend` for up to n_blocks blocks. Returns (outputs, inputs)."""
+    outs, inputs = [], []
+    for _ in range(n_blocks):
+        live = backend.stats().active_voices
+        blk = driver.prepare(live)
+        feed(backend, blk)
+        out = backend.render()
+        outs.append(out.copy())
+        if record:
+            inputs.append(blk)
+        if on_block:
+            on_block(blk, out)
+        if not driver.finish(backend.stats().active_voices):
+            break
+    return outs, inputs
+
+
+# ---- the benchmark configurations --------------------------------------------
+
+def config_workload(name: str, seed: int = 1):
+    """(kc_config, bank spec, midi spec) of a named workload: 'plain' (100k
+    notes, 30 s, 1 preset, 65,536 voices), 'black' (20M notes, 180 s, 128
+    presets, clusters, bend/CC7/CC11 every 10 ms, 1,048,576 voices), 'steal'
+    (200M notes, 120 s, sustained concurrency over an 8,388,608-voice pool,
+    steal-percent 10). Seeded synthetic stand-ins with the shapes the
+    benchmark configurations describe."""
+    if name == "plain":
+        cfg = N.default_config(max_voices=65536)
+        bs = bank_spec(presets=1, seed=seed)
+        ms = midi_spec(notes=100_000, seconds=30.0, dur_median_s=0.150, dur_sigma=1.0, seed=seed)
+    elif name == "black":
+        cfg = N.default_config(max_voices=1_048_576)
+        bs = bank_spec(presets=128, random_generators=1, seed=seed)
+        ms = midi_spec(notes=20_000_000, seconds=180.0, dur_median_s=0.080, dur_sigma=1.0, cluster_share=0.6,
+                       cluster_lo=1000, cluster_hi=50000, cc_period_ms=10.0, program_period_s=2.0, programs=128,
+                       seed=seed)
+    elif name == "steal":
+        cfg = N.default_config(max_voices=8_388_608, max_steal_percent=10)
+        bs = bank_spec(presets=1, seed=seed)
+        ms = midi_spec(notes=200_000_000, seconds=120.0, dur_median_s=6.0, dur_sigma=0.5, seed=seed)
+    else:
+        raise ValueError(f"unknown workload {name!r}")
+    return cfg, bs, ms

@@ -101,6 +101,7 @@ CUDA_SYMBOLS = {
     "kc_synth_create": (C.c_int, [C.POINTER(KcConfig), _P, C.c_uint64, _P, C.c_uint32, C.c_uint32,
                                   C.c_uint32, C.POINTER(_P)]),
     "kc_synth_destroy": (None, [_P]),
+    "kc_synth_clone": (C.c_int, [_P, C.POINTER(_P)]),
     "kc_set_gates": (C.c_int, [_P, _P, C.c_size_t]),
     "kc_set_channels": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int]),
     "kc_set_params_variant": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t]),
@@ -111,6 +112,7 @@ CUDA_SYMBOLS = {
     "kc_set_profile": (C.c_int, [_P, C.c_int]),
     "kc_timings": (C.c_int, [_P, C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.c_size_t,
                              C.POINTER(C.c_size_t)]),
+    "kc_timings_total": (C.c_int, [_P, C.POINTER(C.c_double), C.c_size_t, C.POINTER(C.c_uint64)]),
     "kc_last_error": (C.c_char_p, []),
     "kc_enqueue_block_device": (C.c_int, [_P, _P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_uint32, _P]),
     "kc_synchronize": (C.c_int, [_P]),
