@@ -64,6 +64,8 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the cpu_baseline sample")
+    ap.add_argument("--voices-per-lane", type=int, default=0)
+    ap.add_argument("--strict-fp", type=int, default=1)
     return ap.parse_args(argv)
 
 
@@ -167,6 +169,8 @@ def run_cuda(args, world, rank, local):
     torch.cuda.set_device(local)
     cfg, bs, ms = H.config_workload(args.workload, seed=args.seed + rank)
     cfg.device = local
+    cfg.voices_per_lane = args.voices_per_lane
+    cfg.strict_fp = args.strict_fp
     bank = H.Bank(bs, cfg)
     drv = H.Driver(cfg, bank, ms)
     A = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)

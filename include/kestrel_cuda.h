@@ -140,7 +140,8 @@ typedef struct kc_config {
     uint32_t mix_mode;           /* KC_MIX_*, F32 tree */
     uint32_t strict_fp;          /* 1: no FMA contraction anywhere in the voice DSP */
     uint32_t device;             /* CUDA ordinal */
-    uint32_t reserved[7];
+    uint32_t voices_per_lane;    /* render voices per GPU lane: 0 = default (1), 1 or 2 */
+    uint32_t reserved[6];
 } kc_config;
 
 typedef struct kc_synth kc_synth;

@@ -24,6 +24,7 @@ struct PoolArgs {
     uint32_t admit_rule;
     uint32_t steal_span;
     uint32_t render_warps; // total warps of the render grid
+    uint32_t voices_per_lane;
 };
 
 // ---- admission ---------------------------------------------------------------
@@ -61,7 +62,10 @@ __global__ void k_admit(PoolArgs a, uint32_t* sel_hist, BlockCtl* ctl, uint32_t 
     st->sel_prefix = 0;
     st->sel_k = (uint32_t)need;
     st->peak_bits = 0;
-    const uint32_t nb = (uint32_t)((live + take + 31u) >> 5);
+    // Must match k_render's batching: 32 * voices-per-lane voices per warp.
+    const uint64_t n = live + take;
+    const uint32_t per = 32u * a.voices_per_lane;
+    const uint32_t nb = (uint32_t)((n + per - 1u) / per);
     st->active_warps = nb < a.render_warps ? nb : a.render_warps;
 }
 

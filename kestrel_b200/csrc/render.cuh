@@ -81,9 +81,6 @@ __device__ __forceinline__ uint32_t neighbour(uint32_t idx, int off, bool loopin
     return (uint32_t)(r > hi ? hi : r);
 }
 
-template <bool STRICT>
-__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
-
 struct VoiceRegs {
     uint64_t phase, step, base_step;
     uint32_t base, len, ls, le;
@@ -331,6 +328,56 @@ __device__ __forceinline__ float fast_frame(VoiceRegs& v, const RenderArgs& a, E
     return y;
 }
 
+// The hot path: a tile in which no lane is idle and no envelope transition
+// can happen. `no_transition` is conservative: it proves, with a margin far
+// above the rounding of 16 sequential steps (16 roundings of at most half an
+// ulp each, about 1e-6 relative), that the threshold cannot be crossed inside
+// the tile. When it holds, the frame is branch-free and the compiler can
+// overlap consecutive frames (and the lane's voices).
+__device__ __forceinline__ bool no_transition(const VoiceRegs& v, const EnvStep& e) {
+    if (v.stage == ENV_SUSTAIN) return true;
+    if (v.stage == ENV_ATTACK) {
+        // level grows by attack_rate per frame towards attack_end
+        return v.level + 16.0f * e.ea + 1.0e-5f * fabsf(e.thr) < e.thr;
+    }
+    const float thr = -e.thr;  // decay target or floor
+    if (e.em != 1.0f) {
+        float m = e.em * e.em;  // em^16 by squaring
+        m *= m;
+        m *= m;
+        m *= m;
+        return v.level * m * (1.0f - 1.0e-5f) > thr;
+    }
+    return v.level + 16.0f * e.ea - 1.0e-5f * v.level > thr;  // linear: ea = -coef
+}
+
+template <bool STRICT>
+__device__ __forceinline__ float hot_frame(VoiceRegs& v, const RenderArgs& a, const EnvStep& e) {
+    v.level = __fmaf_rn(v.level, e.em, e.ea);
+    const uint32_t idx = (uint32_t)(v.phase >> 32);
+    const int16_t* p = a.pcm + (v.base + idx);
+    const float s0 = fmaxf(__fmul_rn((float)__ldg(p), 1.0f / 32767.0f), -1.0f);
+    const float s1 = fmaxf(__fmul_rn((float)__ldg(p + 1), 1.0f / 32767.0f), -1.0f);
+    const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
+    const float s = STRICT ? __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac)) : fmaf(s1 - s0, frac, s0);
+    const float x = __fmul_rn(s, fminf(v.level, 1.0f));
+    float y = x;
+    if (v.filt) {
+        if (STRICT) {
+            const float bx = __fmul_rn(v.b0, x);
+            y = __fadd_rn(bx, v.z1);
+            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
+            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
+        } else {
+            y = fmaf(v.b0, x, v.z1);
+            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
+            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
+        }
+    }
+    v.phase += v.step;
+    return y;
+}
+
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
     const float bb = __fsub_rn(s, a);
@@ -341,111 +388,179 @@ constexpr uint32_t RENDER_WARPS = 8;        // warps per CTA
 constexpr uint32_t SM_ROW = 36;             // padded row of the warp tile (floats)
 constexpr uint32_t SM_WARP = 32 * SM_ROW;   // floats per warp tile
 
-// The render pass. Template arguments select the interpolation, whether the
-// channel-controller path is compiled in (the reference builds two pipelines
-// for the same reason, shaders/render.wgsl:36-43), strict rounding, and the
-// mix arithmetic.
-template <int INTERP, bool CHAN, bool STRICT, int MIX>
-__global__ void __launch_bounds__(RENDER_WARPS * 32, 3)
-k_render(RenderArgs a) {
-    extern __shared__ float4 smem4[];
-    float* sm = reinterpret_cast<float*>(smem4) + (threadIdx.x >> 5) * SM_WARP;
+// Load one voice's state into registers (the reference loads the same fields,
+// shaders/render.wgsl:203-237).
+__device__ __forceinline__ void load_voice(VoiceRegs& v, const RenderArgs& a, uint32_t vi, bool live) {
+    v.stage = ENV_DEAD;
+    v.phase = 0; v.step = 0; v.base_step = 0;
+    v.base = 0; v.len = 1; v.ls = 0; v.le = 1;
+    v.level = 0.0f; v.gl = v.gr = v.bgl = v.bgr = 0.0f; v.z1 = v.z2 = 0.0f;
+    v.ar = v.ae = v.dc = v.dt = v.sus = v.rc = v.b0 = v.b1 = v.a1 = v.a2 = 0.0f;
+    v.filt = false; v.loop_en = false; v.lur = false;
+    v.params_base = 0; v.variant = 0; v.born = 0; v.born_gate = 0;
+    v.slot = 0; v.ordinal = 0; v.start_rel = 0; v.stop_rel = 0; v.channel = 0;
+    if (!live) return;
+    const uint32_t cap = a.cap;
+    const uint32_t* P = a.pool + vi;
+    v.phase = ((uint64_t)P[F_PHASE_HI * cap] << 32) | P[F_PHASE_LO * cap];
+    v.base_step = ((uint64_t)P[F_STEP_HI * cap] << 32) | P[F_STEP_LO * cap];
+    v.step = v.base_step;
+    v.base = P[F_SMP_BASE * cap];
+    v.len = P[F_SMP_LEN * cap];
+    v.ls = P[F_LOOP_START * cap];
+    v.le = P[F_LOOP_END * cap];
+    const uint32_t fl = P[F_FLAGS * cap];
+    v.loop_en = (fl & KC_VF_LOOP) != 0u;
+    v.lur = (fl & KC_VF_LOOP_UNTIL_RELEASE) != 0u;
+    v.stage = P[F_ENV_STAGE * cap];
+    v.level = __uint_as_float(P[F_ENV_LEVEL * cap]);
+    v.bgl = __uint_as_float(P[F_GAIN_L * cap]);
+    v.bgr = __uint_as_float(P[F_GAIN_R * cap]);
+    v.gl = v.bgl; v.gr = v.bgr;
+    v.z1 = __uint_as_float(P[F_FILT_Z1 * cap]);
+    v.z2 = __uint_as_float(P[F_FILT_Z2 * cap]);
+    v.params_base = P[F_PARAMS * cap];
+    v.slot = P[F_GATE_SLOT * cap];
+    v.ordinal = P[F_ORDINAL * cap];
+    v.start_rel = P[F_START_REL * cap];
+    v.born = P[F_BORN_VARIANT * cap];
+    v.stop_rel = P[F_STOP_REL * cap];
+    v.variant = v.born ? v.born - 1u : 0u;
+    v.channel = (v.slot >> 7) & 15u;
+    v.born_gate = v.start_rel / a.gate_frames;
+    if (v.params_base >= a.params_per) {
+        atomicOr(&a.st->error, ERR_PARAMS_RANGE);
+        v.params_base = 0;
+    }
+    load_params(v, a, v.variant);
+}
+
+// Write back what a block changes (src/cpu.rs:605-612).
+__device__ __forceinline__ void store_voice(const VoiceRegs& v, const RenderArgs& a, uint32_t vi) {
+    const uint32_t cap = a.cap;
+    uint32_t* P = a.pool + vi;
+    P[F_PHASE_LO * cap] = (uint32_t)v.phase;
+    P[F_PHASE_HI * cap] = (uint32_t)(v.phase >> 32);
+    P[F_ENV_STAGE * cap] = v.stage;
+    P[F_ENV_LEVEL * cap] = __float_as_uint(v.level);
+    P[F_FILT_Z1 * cap] = __float_as_uint(v.z1);
+    P[F_FILT_Z2 * cap] = __float_as_uint(v.z2);
+    P[F_START_REL * cap] = 0u;
+    P[F_BORN_VARIANT * cap] = 0u;
+    P[F_STOP_REL * cap] = 0u;
+}
+
+// Gate and controller rows at the start of a gate tile (src/cpu.rs:450-487).
+template <bool CHAN>
+__device__ __forceinline__ void tile_update(VoiceRegs& v, const RenderArgs& a, uint32_t gt, uint32_t chan_active) {
+    if (v.stage == ENV_DEAD) return;
+    if (v.stage < ENV_RELEASE && __ldg(a.gates + (size_t)gt * KC_GATE_SLOTS + v.slot) >= v.ordinal) {
+        v.stage = ENV_RELEASE;
+        v.level = fminf(v.level, 1.0f);
+    }
+    if (CHAN && chan_active) {
+        const uint4 row = __ldg(reinterpret_cast<const uint4*>(a.chan) + gt * KC_BEND_CHANNELS + v.channel);
+        if (chan_active & 1u) v.step = scale_step(v.base_step, row.x);
+        if (chan_active & 2u) {
+            v.gl = __fmul_rn(v.bgl, __uint_as_float(row.y));
+            v.gr = __fmul_rn(v.bgr, __uint_as_float(row.z));
+        }
+        if (chan_active & 4u) {
+            const bool born_here = v.born != 0u && gt <= v.born_gate;
+            if (row.w != v.variant && !born_here) {
+                v.variant = row.w;
+                load_params(v, a, v.variant);
+            }
+        }
+    }
+}
+
+// Add one voice's frame to the lane's stereo accumulators. The first voice
+// of a lane stores, later ones add in a fixed order.
+template <bool STRICT, bool FIRST>
+__device__ __forceinline__ void acc_out(float& yl, float& yr, float y, const VoiceRegs& v) {
+    if (FIRST) {
+        yl = __fmul_rn(y, v.gl);
+        yr = __fmul_rn(y, v.gr);
+    } else if (STRICT) {
+        yl = __fadd_rn(yl, __fmul_rn(y, v.gl));
+        yr = __fadd_rn(yr, __fmul_rn(y, v.gr));
+    } else {
+        yl = fmaf(y, v.gl, yl);
+        yr = fmaf(y, v.gr, yr);
+    }
+}
+
+// Render every batch of 32*V voices this warp owns. Lane l of batch b holds
+// voices b*32V + k*32 + l for k < V, so each of the V loads per field is one
+// coalesced line, and its V voices' frames are summed in k order before the
+// warp transpose-reduce.
+template <int INTERP, bool CHAN, bool STRICT, int MIX, int V>
+__device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, uint32_t gw, uint32_t tw, uint32_t n) {
     const uint32_t lane = lane_id();
-    const uint32_t gw = blockIdx.x * RENDER_WARPS + (threadIdx.x >> 5);
-    const uint32_t tw = gridDim.x * RENDER_WARPS;
-    const uint32_t n = a.st->live_render;
-    const uint32_t nbatch = (n + 31u) >> 5;
+    const uint32_t per = 32u * V;
+    const uint32_t nbatch = (n + per - 1u) / per;
     const uint32_t samples = a.block_frames * 2u;
     const uint32_t chan_active = CHAN ? a.ctl->chan_active : 0u;
     float* __restrict__ part = a.partial + (size_t)gw * samples;
     float* __restrict__ part_c = MIX ? a.partial_c + (size_t)gw * samples : nullptr;
-    const uint32_t cap = a.cap;
 
     for (uint32_t b = gw; b < nbatch; b += tw) {
-        const uint32_t vi = (b << 5) + lane;
-        const bool live = vi < n;
-        VoiceRegs v;
-        v.stage = ENV_DEAD;
-        v.phase = 0; v.step = 0; v.base_step = 0;
-        v.base = 0; v.len = 1; v.ls = 0; v.le = 1;
-        v.level = 0.0f; v.gl = v.gr = v.bgl = v.bgr = 0.0f; v.z1 = v.z2 = 0.0f;
-        v.ar = v.ae = v.dc = v.dt = v.sus = v.rc = v.b0 = v.b1 = v.a1 = v.a2 = 0.0f;
-        v.filt = false; v.loop_en = false; v.lur = false;
-        v.params_base = 0; v.variant = 0; v.born = 0; v.born_gate = 0;
-        v.slot = 0; v.ordinal = 0; v.start_rel = 0; v.stop_rel = 0; v.channel = 0;
-        if (live) {
-            const uint32_t* P = a.pool + vi;
-            v.phase = ((uint64_t)P[F_PHASE_HI * cap] << 32) | P[F_PHASE_LO * cap];
-            v.base_step = ((uint64_t)P[F_STEP_HI * cap] << 32) | P[F_STEP_LO * cap];
-            v.step = v.base_step;
-            v.base = P[F_SMP_BASE * cap];
-            v.len = P[F_SMP_LEN * cap];
-            v.ls = P[F_LOOP_START * cap];
-            v.le = P[F_LOOP_END * cap];
-            const uint32_t fl = P[F_FLAGS * cap];
-            v.loop_en = (fl & KC_VF_LOOP) != 0u;
-            v.lur = (fl & KC_VF_LOOP_UNTIL_RELEASE) != 0u;
-            v.stage = P[F_ENV_STAGE * cap];
-            v.level = __uint_as_float(P[F_ENV_LEVEL * cap]);
-            v.bgl = __uint_as_float(P[F_GAIN_L * cap]);
-            v.bgr = __uint_as_float(P[F_GAIN_R * cap]);
-            v.gl = v.bgl; v.gr = v.bgr;
-            v.z1 = __uint_as_float(P[F_FILT_Z1 * cap]);
-            v.z2 = __uint_as_float(P[F_FILT_Z2 * cap]);
-            v.params_base = P[F_PARAMS * cap];
-            v.slot = P[F_GATE_SLOT * cap];
-            v.ordinal = P[F_ORDINAL * cap];
-            v.start_rel = P[F_START_REL * cap];
-            v.born = P[F_BORN_VARIANT * cap];
-            v.stop_rel = P[F_STOP_REL * cap];
-            v.variant = v.born ? v.born - 1u : 0u;
-            v.channel = (v.slot >> 7) & 15u;
-            v.born_gate = v.start_rel / a.gate_frames;
-            if (v.params_base >= a.params_per) {
-                atomicOr(&a.st->error, ERR_PARAMS_RANGE);
-                v.params_base = 0;
-            }
-            load_params(v, a, v.variant);
+        VoiceRegs v[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const uint32_t vi = b * per + k * 32u + lane;
+            load_voice(v[k], a, vi, vi < n);
         }
         const bool first = b == gw;
 
         for (uint32_t f0 = 0; f0 < a.block_frames; f0 += MIX_TILE) {
-            if (f0 % a.gate_frames == 0u && v.stage != ENV_DEAD) {
+            if (f0 % a.gate_frames == 0u) {
                 const uint32_t gt = f0 / a.gate_frames;
-                // Note-off gate (src/cpu.rs:450-456).
-                if (v.stage < ENV_RELEASE && __ldg(a.gates + (size_t)gt * KC_GATE_SLOTS + v.slot) >= v.ordinal) {
-                    v.stage = ENV_RELEASE;
-                    v.level = fminf(v.level, 1.0f);
-                }
-                if (CHAN && chan_active) {
-                    // Channel controller path (src/cpu.rs:458-487).
-                    const uint4 row = __ldg(reinterpret_cast<const uint4*>(a.chan) + gt * KC_BEND_CHANNELS + v.channel);
-                    if (chan_active & 1u) v.step = scale_step(v.base_step, row.x);
-                    if (chan_active & 2u) {
-                        v.gl = __fmul_rn(v.bgl, __uint_as_float(row.y));
-                        v.gr = __fmul_rn(v.bgr, __uint_as_float(row.z));
-                    }
-                    if (chan_active & 4u) {
-                        const bool born_here = v.born != 0u && gt <= v.born_gate;
-                        if (row.w != v.variant && !born_here) {
-                            v.variant = row.w;
-                            load_params(v, a, v.variant);
-                        }
-                    }
-                }
+#pragma unroll
+                for (int k = 0; k < V; ++k) tile_update<CHAN>(v[k], a, gt, chan_active);
             }
-            const bool looping = v.loop_en && !(v.lur && v.stage >= ENV_RELEASE);
-            bool active = false;
-            const bool ok = INTERP == KC_INTERP_LINEAR && fast_ok(v, a, f0, looping, active);
-            if (__all_sync(0xFFFFFFFFu, ok)) {
-                EnvStep e = env_constants(v, a);
+            bool looping[V], active[V];
+            bool ok = INTERP == KC_INTERP_LINEAR;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                looping[k] = v[k].loop_en && !(v[k].lur && v[k].stage >= ENV_RELEASE);
+                active[k] = false;
+                if (INTERP == KC_INTERP_LINEAR) ok = fast_ok(v[k], a, f0, looping[k], active[k]) && ok;
+            }
+            EnvStep e[V];
+            bool hot = ok;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                e[k] = env_constants(v[k], a);
+                hot = hot && active[k] && no_transition(v[k], e[k]);
+            }
+            if (__all_sync(0xFFFFFFFFu, hot)) {
+                // Every lane's every voice is live for the whole tile with no
+                // stage change: straight-line code, no branches.
+#pragma unroll
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    float yl, yr;
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        const float y = hot_frame<STRICT>(v[k], a, e[k]);
+                        if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                        else acc_out<STRICT, false>(yl, yr, y, v[k]);
+                    }
+                    sm[(2u * i) * SM_ROW + lane] = yl;
+                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                }
+            } else if (__all_sync(0xFFFFFFFFu, ok)) {
 #pragma unroll
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
                     float yl = 0.0f, yr = 0.0f;
-                    if (active) {
-                        const float y = fast_frame<STRICT>(v, a, e, active);
-                        yl = __fmul_rn(y, v.gl);
-                        yr = __fmul_rn(y, v.gr);
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        if (active[k]) {
+                            const float y = fast_frame<STRICT>(v[k], a, e[k], active[k]);
+                            if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                            else acc_out<STRICT, false>(yl, yr, y, v[k]);
+                        }
                     }
                     sm[(2u * i) * SM_ROW + lane] = yl;
                     sm[(2u * i + 1u) * SM_ROW + lane] = yr;
@@ -455,17 +570,20 @@ k_render(RenderArgs a) {
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
                     const uint32_t f = f0 + i;
                     float yl = 0.0f, yr = 0.0f;
-                    if (v.stage != ENV_DEAD && f >= v.start_rel) {
-                        const float y = voice_frame<INTERP, STRICT>(v, a, f, looping);
-                        yl = __fmul_rn(y, v.gl);
-                        yr = __fmul_rn(y, v.gr);
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        if (v[k].stage != ENV_DEAD && f >= v[k].start_rel) {
+                            const float y = voice_frame<INTERP, STRICT>(v[k], a, f, looping[k]);
+                            if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                            else acc_out<STRICT, false>(yl, yr, y, v[k]);
+                        }
                     }
                     sm[(2u * i) * SM_ROW + lane] = yl;
                     sm[(2u * i + 1u) * SM_ROW + lane] = yr;
                 }
             }
             __syncwarp();
-            // Lane l folds row l (one output slot over the warp's 32 voices).
+            // Lane l folds row l (one output slot over the warp's voices).
             const float4* row = reinterpret_cast<const float4*>(sm + lane * SM_ROW);
             float4 q[8];
 #pragma unroll
@@ -499,20 +617,28 @@ k_render(RenderArgs a) {
                 }
             }
         }
-
-        if (live) {
-            uint32_t* P = a.pool + vi;
-            P[F_PHASE_LO * cap] = (uint32_t)v.phase;
-            P[F_PHASE_HI * cap] = (uint32_t)(v.phase >> 32);
-            P[F_ENV_STAGE * cap] = v.stage;
-            P[F_ENV_LEVEL * cap] = __float_as_uint(v.level);
-            P[F_FILT_Z1 * cap] = __float_as_uint(v.z1);
-            P[F_FILT_Z2 * cap] = __float_as_uint(v.z2);
-            P[F_START_REL * cap] = 0u;
-            P[F_BORN_VARIANT * cap] = 0u;
-            P[F_STOP_REL * cap] = 0u;
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const uint32_t vi = b * per + k * 32u + lane;
+            if (vi < n) store_voice(v[k], a, vi);
         }
     }
+}
+
+// The render pass. Template arguments select the interpolation, whether the
+// channel-controller path is compiled in (the reference builds two pipelines
+// for the same reason, shaders/render.wgsl:36-43), strict rounding, the mix
+// arithmetic, and voices per lane (a per-context setting, so the summation
+// order -- and the output bits -- are a function of the config, the live
+// count and the grid alone).
+template <int INTERP, bool CHAN, bool STRICT, int MIX, int V>
+__global__ void __launch_bounds__(RENDER_WARPS * 32, V == 1 ? 3 : 2)
+k_render(RenderArgs a) {
+    extern __shared__ float4 smem4[];
+    float* sm = reinterpret_cast<float*>(smem4) + (threadIdx.x >> 5) * SM_WARP;
+    const uint32_t gw = blockIdx.x * RENDER_WARPS + (threadIdx.x >> 5);
+    const uint32_t tw = gridDim.x * RENDER_WARPS;
+    render_batches<INTERP, CHAN, STRICT, MIX, V>(a, sm, gw, tw, a.st->live_render);
 }
 
 // Fold the warps' partial slices into the output block in a fixed order:

@@ -65,28 +65,32 @@ SortLayout plan_sort(uint32_t n_regions, uint32_t max_len) {
     return L;
 }
 
-template <int I, bool C, bool S, int M>
+template <int I, bool C, bool S, int M, int V>
 void* render_fn() {
-    return reinterpret_cast<void*>(&k_render<I, C, S, M>);
+    return reinterpret_cast<void*>(&k_render<I, C, S, M, V>);
 }
 
-// Table of render instantiations indexed [interp][chan][strict][mix].
-void* render_table(uint32_t interp, bool chan, bool strict, uint32_t mix) {
-    static void* t[3][2][2][2] = {
-        {{{render_fn<0, false, false, 0>(), render_fn<0, false, false, 1>()},
-          {render_fn<0, false, true, 0>(), render_fn<0, false, true, 1>()}},
-         {{render_fn<0, true, false, 0>(), render_fn<0, true, false, 1>()},
-          {render_fn<0, true, true, 0>(), render_fn<0, true, true, 1>()}}},
-        {{{render_fn<1, false, false, 0>(), render_fn<1, false, false, 1>()},
-          {render_fn<1, false, true, 0>(), render_fn<1, false, true, 1>()}},
-         {{render_fn<1, true, false, 0>(), render_fn<1, true, false, 1>()},
-          {render_fn<1, true, true, 0>(), render_fn<1, true, true, 1>()}}},
-        {{{render_fn<2, false, false, 0>(), render_fn<2, false, false, 1>()},
-          {render_fn<2, false, true, 0>(), render_fn<2, false, true, 1>()}},
-         {{render_fn<2, true, false, 0>(), render_fn<2, true, false, 1>()},
-          {render_fn<2, true, true, 0>(), render_fn<2, true, true, 1>()}}},
-    };
-    return t[interp][chan ? 1 : 0][strict ? 1 : 0][mix ? 1 : 0];
+template <int I, bool C, bool S, int M>
+void* render_v(uint32_t v) {
+    return v == 2 ? render_fn<I, C, S, M, 2>() : render_fn<I, C, S, M, 1>();
+}
+
+template <int I, bool C>
+void* render_sm(bool strict, uint32_t mix, uint32_t v) {
+    if (strict) return mix ? render_v<I, C, true, 1>(v) : render_v<I, C, true, 0>(v);
+    return mix ? render_v<I, C, false, 1>(v) : render_v<I, C, false, 0>(v);
+}
+
+// The render instantiation for [interp][chan][strict][mix][voices per lane].
+void* render_table(uint32_t interp, bool chan, bool strict, uint32_t mix, uint32_t v) {
+    switch (interp) {
+        case KC_INTERP_NEAREST:
+            return chan ? render_sm<0, true>(strict, mix, v) : render_sm<0, false>(strict, mix, v);
+        case KC_INTERP_LINEAR:
+            return chan ? render_sm<1, true>(strict, mix, v) : render_sm<1, false>(strict, mix, v);
+        default:
+            return chan ? render_sm<2, true>(strict, mix, v) : render_sm<2, false>(strict, mix, v);
+    }
 }
 
 }  // namespace
@@ -127,6 +131,7 @@ struct kc_synth {
 
     // launch geometry
     uint32_t render_ctas = 0, render_warps = 0;
+    uint32_t vpl = 1;           // render voices per lane
     size_t render_smem = 0;
     uint32_t pool_ctas = 0;     // grid-stride passes
     uint32_t compact_ctas = 0;  // chunked passes (compaction, sort)
@@ -208,6 +213,7 @@ int validate(const kc_config& c) {
     if (c.steal_rule > 2 || c.admit_rule > 1 || c.interpolation > 2 || c.decay_curve > 1 ||
         c.release_curve > 1 || c.mix_mode > 1)
         return fail(KC_ERR_INVALID, "unknown enum value in config");
+    if (c.voices_per_lane > 2) return fail(KC_ERR_INVALID, "voices_per_lane must be 0, 1 or 2");
     if (c.max_param_variants == 0 || c.max_param_variants > 64)
         return fail(KC_ERR_INVALID, "max_param_variants must be in 1..=64");
     return KC_OK;
@@ -233,6 +239,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     const uint32_t span = c.block_frames > c.steal_fade_frames ? c.block_frames - c.steal_fade_frames : 1;
     pa.steal_span = std::max<uint32_t>(span, 1);
     pa.render_warps = s->render_warps;
+    pa.voices_per_lane = s->vpl;
 
     cudaEvent_t* ev = s->ev;
     if (s->profile) {
@@ -278,7 +285,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     ra.env_floor = c.env_floor;
     ra.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
     ra.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
-    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode);
+    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode, s->vpl);
     void* args[] = {&ra};
     KC_CUDA(cudaLaunchKernel(fn, dim3(s->render_ctas), dim3(RENDER_WARPS * 32), args, s->render_smem, q));
     if (s->profile) cudaEventRecord(ev[3], q);
@@ -409,6 +416,7 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
 
     s->cap = (uint32_t)((slots + 31) & ~31ull);
+    s->vpl = cfg->voices_per_lane == 2 ? 2u : 1u;
     s->tiles = cfg->block_frames / cfg->gate_frames;
     s->params_per = params_len;
     s->n_slots = cfg->max_param_variants;
@@ -420,10 +428,10 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     // Launch geometry: the render grid is every resident CTA of the device,
     // and the partial buffer has one slice per render warp.
     s->render_smem = (size_t)RENDER_WARPS * SM_WARP * sizeof(float);
-    void* fn = render_table(cfg->interpolation, true, cfg->strict_fp != 0, cfg->mix_mode);
+    void* fn = render_table(cfg->interpolation, true, cfg->strict_fp != 0, cfg->mix_mode, s->vpl);
     KC_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->render_smem));
     for (int ch = 0; ch < 2; ++ch) {
-        void* f2 = render_table(cfg->interpolation, ch != 0, cfg->strict_fp != 0, cfg->mix_mode);
+        void* f2 = render_table(cfg->interpolation, ch != 0, cfg->strict_fp != 0, cfg->mix_mode, s->vpl);
         KC_TRY(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->render_smem));
     }
     int per_sm = 0;

@@ -87,13 +87,14 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
                   admit_rule=N.ADMIT_LOUDEST, interpolation=N.INTERP_LINEAR, sort_voices: int = 0,
                   mix_mode=N.MIX_F32_TREE, strict_fp: int = 1, steal_percent: int = 25,
                   release_rate: float = 0.3, unity_step: bool = False, decay_curve=N.CURVE_EXPONENTIAL,
-                  release_curve=N.CURVE_EXPONENTIAL) -> Scenario:
+                  release_curve=N.CURVE_EXPONENTIAL, voices_per_lane: int = 0) -> Scenario:
     rng = np.random.default_rng(seed)
     cfg = N.default_config(max_voices=max_voices, block_frames=block_frames, gate_frames=gate_frames,
                            steal_rule=steal_rule, admit_rule=admit_rule, interpolation=interpolation,
                            sort_voices=sort_voices, mix_mode=mix_mode, strict_fp=strict_fp,
                            max_steal_percent=steal_percent, max_param_variants=max(variants + 1, 1),
-                           decay_curve=decay_curve, release_curve=release_curve)
+                           decay_curve=decay_curve, release_curve=release_curve,
+                           voices_per_lane=voices_per_lane)
     pool, starts, params = make_bank(rng, n_samples, frames, n_params)
     tiles = block_frames // gate_frames
     on_count = np.zeros(N.GATE_SLOTS, np.uint32)

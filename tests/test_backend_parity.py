@@ -50,9 +50,19 @@ def _compare(sc, exact_pool=True, sorted_pool=False, null_limit=-100.0):
 
 
 @gpu
-def test_parity_linear_quietest_chan():
-    sc = make_scenario(seed=1)
+@pytest.mark.parametrize("vpl", [1, 2])
+def test_parity_linear_quietest_chan(vpl):
+    sc = make_scenario(seed=1, voices_per_lane=vpl)
     _compare(sc)
+
+
+@gpu
+@pytest.mark.parametrize("vpl", [1, 2])
+def test_parity_large_pool_sustained(vpl):
+    """Many long-lived voices so most tiles take the branch-free hot path."""
+    sc = make_scenario(seed=12, max_voices=40000, n_blocks=4, spawn_per_block=(9000, 12000), release_rate=0.02,
+                       voices_per_lane=vpl, sort_voices=1)
+    _compare(sc, sorted_pool=True)
 
 
 @gpu
@@ -81,8 +91,9 @@ def test_parity_linear_curves():
 
 
 @gpu
-def test_parity_sorted_pool():
-    sc = make_scenario(seed=8, sort_voices=1)
+@pytest.mark.parametrize("vpl", [1, 2])
+def test_parity_sorted_pool(vpl):
+    sc = make_scenario(seed=8, sort_voices=1, voices_per_lane=vpl)
     _compare(sc, sorted_pool=True)
 
 
