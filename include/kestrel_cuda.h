@@ -221,6 +221,34 @@ void* kc_stream(kc_synth* s);
 /* Number of kernel launches one block enqueues (the captured graph's nodes). */
 int kc_block_launches(kc_synth* s, uint32_t* out);
 
+/* ---- rendering without allocating --------------------------------------- *
+ * No counterpart in the reference. For callers that cannot call cudaMalloc:
+ * allocation can synchronise the whole device and take milliseconds, which a
+ * real-time audio callback cannot wait for, and hosts that manage device
+ * memory themselves (arenas, buffers fixed at start-up) hand every buffer in.
+ * This renders one block of a voice pool the caller owns -- field-major, the
+ * field order of kc_read_pool, `cap` words per field, `n_voices` live -- with
+ * no steal, spawn or compaction, writing block_frames * 2 floats to `d_out`
+ * and updating the voices' state in place. All pointers are device pointers;
+ * `d_params` holds `n_slots` copies of `params_len` entries; `stream` is a
+ * cudaStream_t (NULL: the legacy default stream). The call only enqueues work.
+ *
+ * Its scratch (the partial-mix slices and control words) is a 32 MiB
+ * file-scope device array that every GPU loading this library holds until the
+ * process exits; it bounds a call to 32 voices per 2 * block_frames * 4-byte
+ * slice: 32,736 voices at block_frames 4096 (16,352 with the two-sum mix).
+ * Larger calls are rejected with KC_ERR_INVALID and a message naming the
+ * limit. The first call on a device looks up the array's device address with
+ * that device current; make that first call before any stream capture. Every
+ * call on a device shares the array, so calls that overlap on the GPU race
+ * and must be serialised by the caller. Nothing here calls cudaMalloc,
+ * cudaFree or an allocating library routine. */
+int kc_render_block_noalloc(const kc_config* cfg, uint32_t* d_pool, uint32_t cap, uint32_t n_voices,
+                            const int16_t* d_pcm, uint64_t pcm_len, const kc_region_params* d_params,
+                            uint32_t params_len, uint32_t n_slots, const uint32_t* d_gates,
+                            const uint32_t* d_chan, int bend, int gain, int variant, float* d_out,
+                            void* stream);
+
 /* ---- inspection (tests) ------------------------------------------------- *
  * Copies the live part of the voice pool to the host as 24 SoA fields of
  * `*live` words each (field-major, stride `*live`), in the field order of

@@ -56,7 +56,7 @@ def build_cuda(force: bool = False, extra: list[str] | None = None) -> Path:
         tmp = CUDA_LIB.with_suffix(".so.tmp")
         _run([_nvcc(), *NVCC_ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
               "-Xptxas", "-warn-spills", *(extra or []),
-              str(CSRC / "synth.cu"), "-o", str(tmp)])
+              *[str(p) for p in sorted(CSRC.glob("*.cu"))], "-o", str(tmp)])
         os.replace(tmp, CUDA_LIB)
     return CUDA_LIB
 

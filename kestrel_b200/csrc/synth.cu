@@ -95,6 +95,14 @@ void* render_table(uint32_t interp, bool chan, bool strict, uint32_t mix, uint32
 
 }  // namespace
 
+namespace kc {
+// The error text of the last failing call on this thread, for entry points
+// defined in other files of this library.
+__attribute__((visibility("hidden"))) int set_last_error(int code, const std::string& msg) {
+    return fail(code, msg);
+}
+}  // namespace kc
+
 struct kc_synth {
     kc_config cfg{};
     int device = 0;

@@ -120,6 +120,8 @@ CUDA_SYMBOLS = {
     "kc_stream": (_P, [_P]),
     "kc_block_launches": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "kc_read_pool": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_uint32)]),
+    "kc_render_block_noalloc": (C.c_int, [C.POINTER(KcConfig), _P, C.c_uint32, C.c_uint32, _P, C.c_uint64, _P,
+                                          C.c_uint32, C.c_uint32, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
 }
 
 
