@@ -119,6 +119,7 @@ typedef struct kc_block_stats {
 /* Mixdown arithmetic of the stereo block. */
 #define KC_MIX_F32_TREE 0u     /* fixed-order f32 tree (the reference's device form) */
 #define KC_MIX_TWO_SUM 1u      /* fixed-order tree with compensated two-sum carries */
+#define KC_MIX_F64 2u          /* the f32 voice terms accumulated in f64: an FP64 mix oracle on the device */
 
 /* The subset of config::Config (src/config.rs:164-343) that the backend reads,
  * plus the backend's own tunables. Fill with kc_config_default() first. */
@@ -221,6 +222,17 @@ void* kc_stream(kc_synth* s);
 /* Number of kernel launches one block enqueues (the captured graph's nodes). */
 int kc_block_launches(kc_synth* s, uint32_t* out);
 
+/* ---- precision form ------------------------------------------------------ *
+ * RBJ lowpass coefficients designed in FP64 on the device and rounded once to
+ * f32: `coefs` receives n x (b0, b1, a1, a2) for the n (cutoff Hz, Q in
+ * centibels) pairs, with the arithmetic of biquad_lowpass (src/bank.rs:
+ * 956-979) carried out in double. For regions with a low cutoff or a high Q,
+ * where the reference's f32 design loses most of (1 - cos w0); the caller
+ * patches the returned coefficients into the params table it hands to
+ * kc_synth_create / kc_set_params_variant. Host buffers in and out. */
+int kc_design_lowpass_f64(const float* fc_hz, const float* q_cb, uint32_t n, float sample_rate,
+                          float* coefs, int device);
+
 /* ---- rendering without allocating --------------------------------------- *
  * No counterpart in the reference. For callers that cannot call cudaMalloc:
  * allocation can synchronise the whole device and take milliseconds, which a
@@ -248,6 +260,51 @@ int kc_render_block_noalloc(const kc_config* cfg, uint32_t* d_pool, uint32_t cap
                             uint32_t params_len, uint32_t n_slots, const uint32_t* d_gates,
                             const uint32_t* d_chan, int bend, int gain, int variant, float* d_out,
                             void* stream);
+
+/* ---- batched form --------------------------------------------------------- *
+ * No counterpart in the reference (it renders one file per process). One
+ * kc_batch renders one block of each of up to max_jobs contexts with a single
+ * launch sequence: persistent passes over every job's voices, the render one
+ * persistent kernel over (job, slice) items, captured once as a CUDA graph and
+ * replayed each block. Each job is an ordinary kc_synth whose inputs were set
+ * with kc_set_gates / kc_set_channels / kc_spawn, exactly as before kc_render;
+ * a job's output block, state and stats are byte-identical to rendering that
+ * context alone with kc_render. All jobs must match the batch's device,
+ * block_frames, interpolation, strict_fp, mix_mode and voices_per_lane; the
+ * steal and admit rules, pool sizes, banks and sort setting are per job. */
+typedef struct kc_batch_config {
+    uint32_t device;
+    uint32_t max_jobs;           /* 1..=1024 */
+    uint32_t block_frames;
+    uint32_t interpolation;      /* KC_INTERP_* */
+    uint32_t strict_fp;
+    uint32_t mix_mode;           /* KC_MIX_* */
+    uint32_t voices_per_lane;    /* 0 or 1: one voice per lane; 2: two */
+    uint32_t use_graph;          /* 1: replay a captured graph; 0: launch each pass */
+    uint32_t reserved[8];
+} kc_batch_config;
+
+typedef struct kc_batch kc_batch;
+
+int kc_batch_config_default(kc_batch_config* cfg);
+int kc_batch_create(const kc_batch_config* cfg, kc_batch** out);
+void kc_batch_destroy(kc_batch* b);
+/* One block of each listed job; outs[j] receives block_frames * 2 floats.
+ * Blocks until every output is on the host. A job listed twice, a job of
+ * another variant or more than max_jobs jobs is KC_ERR_INVALID. */
+int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* const* outs);
+/* Device milliseconds of the last kc_batch_render's launch sequence. */
+int kc_batch_last_ms(kc_batch* b, float* ms);
+/* Device memory a context holds, in bytes, and the same figure for a context
+ * not yet created (the serving loop admits jobs by it). */
+uint64_t kc_synth_device_bytes(const kc_synth* s);
+int kc_estimate_device_bytes(const kc_config* cfg, uint64_t pool_len, uint32_t params_len, uint64_t* bytes);
+/* Free and total memory of a device, in bytes. */
+int kc_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
+/* Voices the last completed block rendered: the live voices before its spawn
+ * plus the admitted commands (the per-block term of the voice-samples
+ * metric). */
+int kc_last_block_voices(kc_synth* s, uint32_t* rendered);
 
 /* ---- inspection (tests) ------------------------------------------------- *
  * Copies the live part of the voice pool to the host as 24 SoA fields of

@@ -87,6 +87,10 @@ uint32_t kh_bank_regions(const kh_bank* b);
 uint32_t kh_bank_presets(const kh_bank* b);
 uint32_t kh_bank_max_sample_len(const kh_bank* b);
 uint32_t kh_bank_pool_rate(const kh_bank* b);
+/* Per entry of the variant-0 params table: the cutoff (Hz) and Q (cB) its
+ * lowpass was designed from and whether the filter is on (make_params,
+ * src/bank.rs:918-938). Each array holds kh_bank_params' length. */
+int kh_bank_filter_inputs(const kh_bank* b, float* fc_hz, float* q_cb, uint8_t* on, uint32_t n);
 
 /* ---- synthetic MIDI ------------------------------------------------------ */
 

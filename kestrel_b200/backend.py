@@ -149,3 +149,63 @@ class CudaSynth:
         N.check(self._lib.kc_read_pool(self._h, N.ptr(buf), buf.size, C.byref(live)), self._lib)
         n = live.value
         return buf[: 24 * n].reshape(24, n).copy()
+
+    def device_bytes(self) -> int:
+        """Device memory this context holds (kc_synth_device_bytes)."""
+        return int(self._lib.kc_synth_device_bytes(self._h))
+
+    def last_block_voices(self) -> int:
+        """Voices the last block rendered (live before spawn + admitted)."""
+        n = C.c_uint32()
+        N.check(self._lib.kc_last_block_voices(self._h, C.byref(n)), self._lib)
+        return n.value
+
+
+class CudaBatch:
+    """One block of many contexts per call (kc_batch_render).
+
+    Each job is a CudaSynth whose inputs were set with set_gates /
+    set_channels / spawn, exactly as before CudaSynth.render; after
+    render(jobs) every job's output, state and stats are those of rendering it
+    alone.
+    """
+
+    def __init__(self, cfg: N.KcBatchConfig):
+        self._lib = N.cuda_lib()
+        self.cfg = cfg
+        h = C.c_void_p()
+        N.check(self._lib.kc_batch_create(C.byref(cfg), C.byref(h)), self._lib)
+        self._h = h
+        self.block_frames = cfg.block_frames
+
+    @classmethod
+    def for_config(cls, cfg: N.KcConfig, max_jobs: int = 256, use_graph: bool = True) -> "CudaBatch":
+        return cls(N.batch_config_for(cfg, max_jobs, use_graph))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.kc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def render(self, jobs: list[CudaSynth], outs: list[np.ndarray] | None = None) -> list[np.ndarray]:
+        n = len(jobs)
+        if outs is None:
+            outs = [np.empty(self.block_frames * 2, dtype=np.float32) for _ in range(n)]
+        hs = (C.c_void_p * max(n, 1))(*[j._h.value for j in jobs])
+        ps = (C.c_void_p * max(n, 1))(*[N.ptr(o) for o in outs])
+        N.check(self._lib.kc_batch_render(self._h, hs, n, ps), self._lib)
+        return outs
+
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        N.check(self._lib.kc_batch_last_ms(self._h, C.byref(ms)), self._lib)
+        return ms.value

@@ -5,6 +5,9 @@
 * ``kestrel_b200/libkestrel_host.so``: the host-side driver that produces the
   backend's per-block inputs (bank, MIDI timeline, gate/channel tables,
   admission), C++17.
+* ``kestrel_b200/libkestrel_serve.so``: the render server (continuous
+  batching over kc_batch_render, or the plain path one job at a time), C++17,
+  linked against the two libraries above.
 * ``oracle/liboracle.so``: the CPU restatement of the reference backend, the
   checker used only by the tests and the CPU-baseline legs of the benchmark.
 
@@ -27,6 +30,7 @@ INCLUDE = ROOT / "include"
 CUDA_LIB = PKG / "libkestrel_cuda.so"
 HOST_LIB = PKG / "libkestrel_host.so"
 ORACLE_LIB = ORACLE / "liboracle.so"
+SERVE_LIB = PKG / "libkestrel_serve.so"
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -75,6 +79,20 @@ def build_host(force: bool = False) -> Path:
     return HOST_LIB
 
 
+def build_serve(force: bool = False) -> Path:
+    """The render server: links the CUDA backend and the host library."""
+    sdir = CSRC / "serve"
+    srcs = sorted(sdir.glob("*.cpp")) + [INCLUDE / "kestrel_serve.h", INCLUDE / "kestrel_cuda.h",
+                                         INCLUDE / "kestrel_host.h", CUDA_LIB, HOST_LIB]
+    if force or _stale(SERVE_LIB, srcs):
+        tmp = SERVE_LIB.with_suffix(".so.tmp")
+        _run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-pthread",
+              *[str(p) for p in sorted(sdir.glob("*.cpp"))], f"-L{PKG}", "-lkestrel_cuda", "-lkestrel_host",
+              "-Wl,-rpath,$ORIGIN", "-o", str(tmp)])
+        os.replace(tmp, SERVE_LIB)
+    return SERVE_LIB
+
+
 def build_oracle(force: bool = False) -> Path:
     srcs = sorted(ORACLE.glob("*.cpp")) + sorted(ORACLE.glob("*.h")) + [INCLUDE / "kestrel_cuda.h"]
     if force or _stale(ORACLE_LIB, srcs):
@@ -89,6 +107,7 @@ def build_all(force: bool = False) -> None:
     build_host(force)
     build_oracle(force)
     build_cuda(force)
+    build_serve(force)
 
 
 if __name__ == "__main__":

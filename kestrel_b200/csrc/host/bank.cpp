@@ -351,6 +351,31 @@ std::vector<kc_region_params> Bank::build_variant(const BankConfig& cfg, const P
     return out;
 }
 
+void Bank::filter_inputs(const BankConfig& cfg, const ParamMod& m, std::vector<float>& fc, std::vector<float>& q_cb,
+                         std::vector<uint8_t>& on) const {
+    const float sr = (float)cfg.sample_rate;
+    fc.clear();
+    q_cb.clear();
+    on.clear();
+    auto one = [&](const Region& r, uint8_t vel) {
+        // make_params, src/bank.rs:922-938: the cutoff, its guard, and the Q.
+        const float fc_cents = r.filter_fc_cents + r.filter_veltrack_cents * ((float)vel / 127.0f) + m.cutoff_cents;
+        const float f = cents_to_hz(fc_cents);
+        const bool use = cfg.filter_enabled && fc_cents < 13500.0f && f < sr * 0.49f && f > 20.0f;
+        fc.push_back(f);
+        q_cb.push_back(r.filter_q_cb + m.q_cb);
+        on.push_back(use ? 1 : 0);
+    };
+    for (const auto& r : regions) {
+        const bool per_key = r.params_stride != 0;
+        for (uint32_t v = 0; v < r.params_vel_span; ++v) {
+            const uint8_t vel = (uint8_t)std::min<uint32_t>(r.vel_lo + v, 127);
+            const int reps = per_key ? 128 : 1;
+            for (int k = 0; k < reps; ++k) one(r, vel);
+        }
+    }
+}
+
 uint32_t Bank::max_sample_len() const {
     uint32_t m = 1;
     for (const auto& s : samples) m = std::max(m, s.len);

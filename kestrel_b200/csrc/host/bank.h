@@ -108,6 +108,10 @@ struct Bank {
     void preview_note_on(uint32_t preset, uint8_t key, uint8_t vel, size_t max_layers,
                          std::vector<PreviewLayer>& out) const;
     std::vector<kc_region_params> build_variant(const BankConfig& cfg, const ParamMod& m) const;
+    // The (cutoff Hz, Q cB, filter on) each entry of build_variant's table was
+    // designed from, in the same order.
+    void filter_inputs(const BankConfig& cfg, const ParamMod& m, std::vector<float>& fc, std::vector<float>& q_cb,
+                       std::vector<uint8_t>& on) const;
     uint32_t max_sample_len() const;
 };
 

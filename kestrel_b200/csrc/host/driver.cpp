@@ -620,6 +620,7 @@ using namespace kh;
 
 struct kh_bank {
     Bank bank;
+    BankConfig cfg;
 };
 struct kh_driver {
     std::unique_ptr<Driver> d;
@@ -674,6 +675,7 @@ kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg,
     b.resample_pool = o.resample_pool != 0;
     b.sample_pool_budget = o.sample_pool_budget;
     auto* kb = new kh_bank();
+    kb->cfg = b;
     if (!load_sf2(synth_sf2(*spec), b, &kb->bank, &g_err)) {
         delete kb;
         return nullptr;
@@ -697,6 +699,20 @@ uint32_t kh_bank_regions(const kh_bank* b) { return (uint32_t)b->bank.regions.si
 uint32_t kh_bank_presets(const kh_bank* b) { return (uint32_t)b->bank.presets.size(); }
 uint32_t kh_bank_max_sample_len(const kh_bank* b) { return b->bank.max_sample_len(); }
 uint32_t kh_bank_pool_rate(const kh_bank* b) { return b->bank.pool_rate; }
+
+int kh_bank_filter_inputs(const kh_bank* b, float* fc_hz, float* q_cb, uint8_t* on, uint32_t n) {
+    std::vector<float> f, q;
+    std::vector<uint8_t> o;
+    b->bank.filter_inputs(b->cfg, ParamMod{}, f, q, o);
+    if (n != f.size()) {
+        g_err = "filter inputs: expected one slot per params entry";
+        return 1;
+    }
+    std::memcpy(fc_hz, f.data(), n * 4);
+    std::memcpy(q_cb, q.data(), n * 4);
+    std::memcpy(on, o.data(), n);
+    return 0;
+}
 
 void kh_midi_spec_default(kh_midi_spec* s) {
     std::memset(s, 0, sizeof(*s));

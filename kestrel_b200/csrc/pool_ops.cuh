@@ -30,11 +30,7 @@ struct PoolArgs {
 // ---- admission ---------------------------------------------------------------
 // The spawn arithmetic of CpuSynth::spawn (src/cpu.rs:330-390), on the device
 // so the live count never has to come back to the host between blocks.
-__global__ void k_admit(PoolArgs a, uint32_t* sel_hist, BlockCtl* ctl, uint32_t want32,
-                        uint32_t chan_active) {
-    const uint32_t t = threadIdx.x;
-    for (uint32_t i = t; i < SEL_ROUNDS * 256u; i += blockDim.x) sel_hist[i] = 0u;
-    if (t != 0) return;
+__device__ __forceinline__ void admit_state(PoolArgs a, BlockCtl* ctl, uint32_t want32, uint32_t chan_active) {
     ctl->want = want32;
     ctl->chan_active = chan_active;
     DevState* st = a.st;
@@ -89,7 +85,8 @@ __device__ __forceinline__ uint64_t steal_key(const uint32_t* pool, uint32_t cap
     return (q << 48) | (id & 0x0000FFFFFFFFFFFFull);
 }
 
-__global__ void __launch_bounds__(256) k_select_hist(PoolArgs a, uint32_t* sel_hist, uint32_t round) {
+__device__ __forceinline__ void select_hist_body(PoolArgs a, uint32_t* sel_hist, uint32_t round, uint32_t cta,
+                                                 uint32_t ctas) {
     __shared__ uint32_t h[256];
     const DevState* st = a.st;
     if (st->need == 0) return;
@@ -99,7 +96,7 @@ __global__ void __launch_bounds__(256) k_select_hist(PoolArgs a, uint32_t* sel_h
     const uint32_t b = 7u - round;              // byte index, MSB first
     const uint64_t prefix = st->sel_prefix;
     const uint32_t hs = 8u * (b + 1u);          // bits above this byte
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = cta * blockDim.x + threadIdx.x; i < n; i += ctas * blockDim.x) {
         const uint64_t k = steal_key(a.pool, a.cap, i, a.steal_rule);
         if (hs >= 64u || (k >> hs) == (prefix >> hs)) atomicAdd(&h[(uint32_t)(k >> (8u * b)) & 255u], 1u);
     }
@@ -109,7 +106,7 @@ __global__ void __launch_bounds__(256) k_select_hist(PoolArgs a, uint32_t* sel_h
 }
 
 // Pin one byte: the bin where the running count reaches k. One CTA of 256.
-__global__ void __launch_bounds__(256) k_select_refine(PoolArgs a, const uint32_t* sel_hist, uint32_t round) {
+__device__ __forceinline__ void select_refine_body(PoolArgs a, const uint32_t* sel_hist, uint32_t round) {
     __shared__ uint32_t scan[256];
     DevState* st = a.st;
     if (st->need == 0) return;
@@ -138,12 +135,12 @@ __global__ void __launch_bounds__(256) k_select_refine(PoolArgs a, const uint32_
 // Schedule each victim's fade (src/cpu.rs:360-371; shaders/compact.wgsl:
 // 263-291): stop_rel = (note id low word) % span + 1. Only the pre-spawn
 // voices are candidates.
-__global__ void __launch_bounds__(256) k_mark_stolen(PoolArgs a) {
+__device__ __forceinline__ void mark_stolen_body(PoolArgs a, uint32_t cta, uint32_t ctas) {
     const DevState* st = a.st;
     if (st->need == 0) return;
     const uint32_t n = st->live_old;
     const uint64_t thresh = st->sel_prefix;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = cta * blockDim.x + threadIdx.x; i < n; i += ctas * blockDim.x) {
         if (steal_key(a.pool, a.cap, i, a.steal_rule) <= thresh) {
             const uint32_t lo = a.pool[F_NOTE_LO * a.cap + i];
             a.pool[F_STOP_REL * a.cap + i] = lo % a.steal_span + 1u;
@@ -158,7 +155,8 @@ __global__ void __launch_bounds__(256) k_mark_stolen(PoolArgs a) {
 // src/voice.rs:71-75). One warp handles 32 commands: it stages their 76-byte
 // records through shared memory so both the read of the command array and the
 // 24 field rows of the pool are written with full coalescing.
-__global__ void __launch_bounds__(256) k_spawn(PoolArgs a, const kc_spawn_cmd* __restrict__ cmds) {
+__device__ __forceinline__ void spawn_body(PoolArgs a, const kc_spawn_cmd* __restrict__ cmds, uint32_t cta,
+                                           uint32_t ctas) {
     __shared__ uint32_t stage[8][32 * 19 + 1];
     const DevState* st = a.st;
     const uint32_t take = st->take;
@@ -166,7 +164,7 @@ __global__ void __launch_bounds__(256) k_spawn(PoolArgs a, const kc_spawn_cmd* _
     const uint32_t want = a.ctl->want;
     const uint32_t base = st->live_old;
     const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    const uint32_t gw = blockIdx.x * 8u + w, tw = gridDim.x * 8u;
+    const uint32_t gw = cta * 8u + w, tw = ctas * 8u;
     uint32_t* s = stage[w];
     for (uint32_t g = gw; g * 32u < take; g += tw) {
         const uint32_t i0 = g * 32u;
@@ -226,11 +224,11 @@ __device__ __forceinline__ uint32_t compact_chunk(uint32_t n, uint32_t nblocks) 
     return (c + 255u) & ~255u;
 }
 
-__global__ void __launch_bounds__(256) k_compact_count(PoolArgs a, uint32_t* counts) {
+__device__ __forceinline__ void compact_count_body(PoolArgs a, uint32_t* counts, uint32_t cta, uint32_t ctas) {
     __shared__ uint32_t wsum[8];
     const uint32_t n = a.st->live_render;
-    const uint32_t chunk = compact_chunk(n, gridDim.x);
-    const uint32_t lo = blockIdx.x * chunk;
+    const uint32_t chunk = compact_chunk(n, ctas);
+    const uint32_t lo = cta * chunk;
     const uint32_t hi = min(n, lo + chunk);
     uint32_t c = 0;
     for (uint32_t i = lo + threadIdx.x; i < hi; i += 256u) c += a.pool[F_ENV_STAGE * a.cap + i] != ENV_DEAD;
@@ -240,12 +238,12 @@ __global__ void __launch_bounds__(256) k_compact_count(PoolArgs a, uint32_t* cou
     if (threadIdx.x == 0) {
         uint32_t t = 0;
         for (int k = 0; k < 8; ++k) t += wsum[k];
-        counts[blockIdx.x] = t;
+        counts[cta] = t;
     }
 }
 
 // Exclusive scan of the per-CTA counts (any count of CTAs), one CTA of 1024.
-__global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* counts, uint32_t m, uint32_t* total) {
+__device__ __forceinline__ void scan_counts_body(uint32_t* counts, uint32_t m, uint32_t* total) {
     __shared__ uint32_t wsum[32];
     __shared__ uint32_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -290,14 +288,15 @@ __device__ __forceinline__ void copy_voice(const uint32_t* src, uint32_t* dst, u
     dst[F_STOP_REL * cap + to] = 0u;
 }
 
-__global__ void __launch_bounds__(256) k_compact_scatter(PoolArgs a, const uint32_t* offsets) {
+__device__ __forceinline__ void compact_scatter_body(PoolArgs a, const uint32_t* offsets, uint32_t cta,
+                                                     uint32_t ctas) {
     __shared__ uint32_t wsum[8];
     const uint32_t n = a.st->live_render;
-    const uint32_t chunk = compact_chunk(n, gridDim.x);
-    const uint32_t lo = blockIdx.x * chunk;
+    const uint32_t chunk = compact_chunk(n, ctas);
+    const uint32_t lo = cta * chunk;
     const uint32_t hi = min(n, lo + chunk);
     const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    uint32_t run = offsets[blockIdx.x];
+    uint32_t run = offsets[cta];
     for (uint32_t t0 = lo; t0 < hi; t0 += 256u) {
         const uint32_t i = t0 + threadIdx.x;
         const bool alive = i < hi && a.pool[F_ENV_STAGE * a.cap + i] != ENV_DEAD;
@@ -318,7 +317,7 @@ __global__ void __launch_bounds__(256) k_compact_scatter(PoolArgs a, const uint3
     }
 }
 
-__global__ void k_commit(DevState* st, const uint32_t* total) {
+__device__ __forceinline__ void commit_body(DevState* st, const uint32_t* total) {
     st->live_new = *total;
     st->live = *total;
 }
@@ -353,36 +352,35 @@ __device__ __forceinline__ uint32_t sort_chunk(uint32_t n, uint32_t nblocks) {
 
 // Pass `shift`: count digit occurrences per CTA chunk into counts[d * G + cta].
 // Pass 0 computes keys from the pool; later passes read the key array.
-__global__ void __launch_bounds__(256) k_sort_count(PoolArgs a, SortLayout L, const uint32_t* keys,
-                                                    uint32_t shift, uint32_t* counts) {
+__device__ __forceinline__ void sort_count_body(PoolArgs a, SortLayout L, const uint32_t* keys, uint32_t shift,
+                                                uint32_t* counts, uint32_t cta, uint32_t ctas) {
     __shared__ uint32_t h[256];
     const uint32_t n = a.st->live_render;
     h[threadIdx.x] = 0u;
     __syncthreads();
-    const uint32_t chunk = sort_chunk(n, gridDim.x);
-    const uint32_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    const uint32_t chunk = sort_chunk(n, ctas);
+    const uint32_t lo = cta * chunk, hi = min(n, lo + chunk);
     for (uint32_t i = lo + threadIdx.x; i < hi; i += 256u) {
         const uint32_t k = keys ? keys[i] : sort_key(a.pool, a.cap, i, L);
         atomicAdd(&h[(k >> shift) & 255u], 1u);
     }
     __syncthreads();
-    counts[threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
+    counts[threadIdx.x * ctas + cta] = h[threadIdx.x];
 }
 
 // Stable scatter of one pass. keys_in == nullptr on the first pass (keys and
 // indices come from the pool order).
-__global__ void __launch_bounds__(256) k_sort_scatter(PoolArgs a, SortLayout L, const uint32_t* keys_in,
+__device__ __forceinline__ void sort_scatter_body(PoolArgs a, SortLayout L, const uint32_t* keys_in,
                                                       const uint32_t* idx_in, uint32_t* keys_out,
                                                       uint32_t* idx_out, uint32_t shift,
-                                                      const uint32_t* offsets) {
+                                                      const uint32_t* offsets, uint32_t cta, uint32_t ctas) {
     __shared__ uint32_t run[256];
     __shared__ uint32_t wcnt[8][256];
     const uint32_t n = a.st->live_render;
-    const uint32_t G = gridDim.x;
     const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    run[threadIdx.x] = offsets[threadIdx.x * G + blockIdx.x];
-    const uint32_t chunk = sort_chunk(n, G);
-    const uint32_t lo = blockIdx.x * chunk, hi = min(n, lo + chunk);
+    run[threadIdx.x] = offsets[threadIdx.x * ctas + cta];
+    const uint32_t chunk = sort_chunk(n, ctas);
+    const uint32_t lo = cta * chunk, hi = min(n, lo + chunk);
     for (uint32_t t0 = lo; t0 < hi; t0 += 256u) {
         for (uint32_t k = 0; k < 8; ++k) wcnt[k][threadIdx.x] = 0u;
         __syncthreads();
@@ -417,9 +415,9 @@ __global__ void __launch_bounds__(256) k_sort_scatter(PoolArgs a, SortLayout L, 
 // (k_scan_counts handles it: it is a plain exclusive scan of m words.)
 
 // Copy the sorted survivors into the other pool buffer.
-__global__ void __launch_bounds__(256) k_sort_gather(PoolArgs a, const uint32_t* idx) {
+__device__ __forceinline__ void sort_gather_body(PoolArgs a, const uint32_t* idx, uint32_t cta, uint32_t ctas) {
     const uint32_t n = a.st->live_new;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    for (uint32_t j = cta * blockDim.x + threadIdx.x; j < n; j += ctas * blockDim.x)
         copy_voice(a.pool, a.pool_out, a.cap, idx[j], j);
 }
 

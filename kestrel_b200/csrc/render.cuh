@@ -378,6 +378,35 @@ __device__ __forceinline__ float hot_frame(VoiceRegs& v, const RenderArgs& a, co
     return y;
 }
 
+// The hot path when every lane's phase and step have a zero fraction (an
+// exactly integer pitch ratio: the root key played at the pool rate, or whole
+// octaves of it). Then frac is 0 for every frame of the tile, and the linear
+// interpolation s0 + (s1 - s0) * 0 is exactly s0 (s0 is never -0: it is
+// v / 32767 clamped at -1, so +0 for a zero tap), in both the strict and the
+// fused form. The second tap, its conversion and the lerp drop out.
+template <bool STRICT>
+__device__ __forceinline__ float hot_frame_int(VoiceRegs& v, const RenderArgs& a, const EnvStep& e) {
+    v.level = __fmaf_rn(v.level, e.em, e.ea);
+    const uint32_t idx = (uint32_t)(v.phase >> 32);
+    const float s = fmaxf(__fmul_rn((float)__ldg(a.pcm + (v.base + idx)), 1.0f / 32767.0f), -1.0f);
+    const float x = __fmul_rn(s, fminf(v.level, 1.0f));
+    float y = x;
+    if (v.filt) {
+        if (STRICT) {
+            const float bx = __fmul_rn(v.b0, x);
+            y = __fadd_rn(bx, v.z1);
+            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
+            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
+        } else {
+            y = fmaf(v.b0, x, v.z1);
+            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
+            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
+        }
+    }
+    v.phase += v.step;  // the fraction stays zero
+    return y;
+}
+
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
     const float bb = __fsub_rn(s, a);
@@ -503,7 +532,10 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
     const uint32_t samples = a.block_frames * 2u;
     const uint32_t chan_active = CHAN ? a.ctl->chan_active : 0u;
     float* __restrict__ part = a.partial + (size_t)gw * samples;
-    float* __restrict__ part_c = MIX ? a.partial_c + (size_t)gw * samples : nullptr;
+    float* __restrict__ part_c = MIX == KC_MIX_TWO_SUM ? a.partial_c + (size_t)gw * samples : nullptr;
+    // KC_MIX_F64: the same buffer holds one slice of doubles per warp.
+    double* __restrict__ part_d = MIX == KC_MIX_F64 ? reinterpret_cast<double*>(a.partial) + (size_t)gw * samples
+                                                    : nullptr;
 
     for (uint32_t b = gw; b < nbatch; b += tw) {
         VoiceRegs v[V];
@@ -535,7 +567,24 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 e[k] = env_constants(v[k], a);
                 hot = hot && active[k] && no_transition(v[k], e[k]);
             }
-            if (__all_sync(0xFFFFFFFFu, hot)) {
+            bool integral = true;
+#pragma unroll
+            for (int k = 0; k < V; ++k) integral = integral && ((uint32_t)v[k].phase | (uint32_t)v[k].step) == 0u;
+            if (INTERP == KC_INTERP_LINEAR && __all_sync(0xFFFFFFFFu, hot && integral)) {
+                // Straight-line frames with a zero phase fraction.
+#pragma unroll
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    float yl, yr;
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        const float y = hot_frame_int<STRICT>(v[k], a, e[k]);
+                        if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                        else acc_out<STRICT, false>(yl, yr, y, v[k]);
+                    }
+                    sm[(2u * i) * SM_ROW + lane] = yl;
+                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                }
+            } else if (__all_sync(0xFFFFFFFFu, hot)) {
                 // Every lane's every voice is live for the whole tile with no
                 // stage change: straight-line code, no branches.
 #pragma unroll
@@ -597,6 +646,14 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 const float sum = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
                                             __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
                 part[j] = first ? sum : __fadd_rn(part[j], sum);
+            } else if (MIX == KC_MIX_F64) {
+                // The FP64 form: the row's 32 f32 terms summed in double.
+                double r[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    r[c] = ((double)q[c].x + (double)q[c].y) + ((double)q[c].z + (double)q[c].w);
+                const double sum = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+                part_d[j] = first ? sum : part_d[j] + sum;
             } else {
                 // Compensated: sequential two-sum over the row with carries.
                 float s = q[0].x, e = 0.0f, t, err;
@@ -645,15 +702,32 @@ k_render(RenderArgs a) {
 // warp k of the CTA sums slices k, k+8, ... for 32 consecutive samples, then
 // warp 0 adds the eight in order. Also records max |out| for BlockStats::peak.
 template <int MIX>
-__global__ void __launch_bounds__(256) k_reduce(const float* __restrict__ partial,
+__device__ __forceinline__ void reduce_body(const float* __restrict__ partial,
                                                 const float* __restrict__ partial_c,
                                                 float* __restrict__ out, DevState* st,
-                                                uint32_t samples) {
+                                                uint32_t samples, uint32_t cta) {
     __shared__ float red[8][32];
     __shared__ float redc[8][32];
+    __shared__ double redd[8][32];
     const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    const uint32_t j = blockIdx.x * 32u + lane;
+    const uint32_t j = cta * 32u + lane;
     const uint32_t nw = st->active_warps;
+    if (MIX == KC_MIX_F64) {
+        const double* pd = reinterpret_cast<const double*>(partial);
+        double d = 0.0;
+        if (j < samples)
+            for (uint32_t k = w; k < nw; k += 8u) d += __ldcs(pd + (size_t)k * samples + j);
+        redd[w][lane] = d;
+        __syncthreads();
+        if (w == 0 && j < samples) {
+            double tot = redd[0][lane];
+            for (int k = 1; k < 8; ++k) tot += redd[k][lane];
+            const float f = (float)tot;
+            out[j] = f;
+            atomicMax(&st->peak_bits, __float_as_uint(fabsf(f)));
+        }
+        return;
+    }
     float s = 0.0f, e = 0.0f;
     if (j < samples) {
         for (uint32_t k = w; k < nw; k += 8u) {
@@ -688,6 +762,14 @@ __global__ void __launch_bounds__(256) k_reduce(const float* __restrict__ partia
         // |x| of a finite float orders like its bit pattern.
         atomicMax(&st->peak_bits, __float_as_uint(fabsf(tot)));
     }
+}
+
+template <int MIX>
+__global__ void __launch_bounds__(256) k_reduce(const float* __restrict__ partial,
+                                                const float* __restrict__ partial_c,
+                                                float* __restrict__ out, DevState* st,
+                                                uint32_t samples) {
+    reduce_body<MIX>(partial, partial_c, out, st, samples, blockIdx.x);
 }
 
 }  // namespace kc

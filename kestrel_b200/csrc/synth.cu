@@ -18,6 +18,56 @@
 #include "common.cuh"
 #include "pool_ops.cuh"
 #include "render.cuh"
+#include "synth_impl.cuh"
+
+// The single-context kernels: each runs one pass body (pool_ops.cuh) over
+// this launch's own grid.
+namespace kc {
+
+__global__ void k_admit(PoolArgs a, uint32_t* sel_hist, BlockCtl* ctl, uint32_t want32, uint32_t chan_active) {
+    for (uint32_t i = threadIdx.x; i < SEL_ROUNDS * 256u; i += blockDim.x) sel_hist[i] = 0u;
+    if (threadIdx.x == 0) admit_state(a, ctl, want32, chan_active);
+}
+
+__global__ void __launch_bounds__(256) k_select_hist(PoolArgs a, uint32_t* sel_hist, uint32_t round) {
+    select_hist_body(a, sel_hist, round, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(256) k_select_refine(PoolArgs a, const uint32_t* sel_hist, uint32_t round) { select_refine_body(a, sel_hist, round); }
+
+__global__ void __launch_bounds__(256) k_mark_stolen(PoolArgs a) { mark_stolen_body(a, blockIdx.x, gridDim.x); }
+
+__global__ void __launch_bounds__(256) k_spawn(PoolArgs a, const kc_spawn_cmd* __restrict__ cmds) {
+    spawn_body(a, cmds, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(256) k_compact_count(PoolArgs a, uint32_t* counts) {
+    compact_count_body(a, counts, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(1024) k_scan_counts(uint32_t* counts, uint32_t m, uint32_t* total) { scan_counts_body(counts, m, total); }
+
+__global__ void __launch_bounds__(256) k_compact_scatter(PoolArgs a, const uint32_t* offsets) {
+    compact_scatter_body(a, offsets, blockIdx.x, gridDim.x);
+}
+
+__global__ void k_commit(DevState* st, const uint32_t* total) { commit_body(st, total); }
+
+__global__ void __launch_bounds__(256) k_sort_count(PoolArgs a, SortLayout L, const uint32_t* keys,
+                                                    uint32_t shift, uint32_t* counts) {
+    sort_count_body(a, L, keys, shift, counts, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(256) k_sort_scatter(PoolArgs a, SortLayout L, const uint32_t* keys_in,
+                                                      const uint32_t* idx_in, uint32_t* keys_out,
+                                                      uint32_t* idx_out, uint32_t shift,
+                                                      const uint32_t* offsets) {
+    sort_scatter_body(a, L, keys_in, idx_in, keys_out, idx_out, shift, offsets, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(256) k_sort_gather(PoolArgs a, const uint32_t* idx) { sort_gather_body(a, idx, blockIdx.x, gridDim.x); }
+
+}  // namespace kc
 
 using namespace kc;
 
@@ -37,8 +87,7 @@ int fail(int code, const std::string& msg) {
             return fail(KC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-constexpr int N_TIMERS = 5;
-const char* kPassNames[N_TIMERS] = {"steal", "spawn", "render", "reduce", "compact"};
+const char* kPassNames[kc::N_TIMERS] = {"steal", "spawn", "render", "reduce", "compact"};
 
 uint32_t max_steal_of(const kc_config& c) {
     const uint64_t n = (uint64_t)c.max_voices * c.max_steal_percent / 100;
@@ -70,15 +119,25 @@ void* render_fn() {
     return reinterpret_cast<void*>(&k_render<I, C, S, M, V>);
 }
 
+// Two voices per lane is instantiated for the linear interpolator and the
+// f32 mix only (the combinations the autotuner chooses between).
 template <int I, bool C, bool S, int M>
 void* render_v(uint32_t v) {
-    return v == 2 ? render_fn<I, C, S, M, 2>() : render_fn<I, C, S, M, 1>();
+    if constexpr (I == KC_INTERP_LINEAR && M == KC_MIX_F32_TREE)
+        if (v == 2) return render_fn<I, C, S, M, 2>();
+    return render_fn<I, C, S, M, 1>();
+}
+
+template <int I, bool C, bool S>
+void* render_m(uint32_t mix, uint32_t v) {
+    if (mix == KC_MIX_TWO_SUM) return render_v<I, C, S, KC_MIX_TWO_SUM>(v);
+    if (mix == KC_MIX_F64) return render_v<I, C, S, KC_MIX_F64>(v);
+    return render_v<I, C, S, KC_MIX_F32_TREE>(v);
 }
 
 template <int I, bool C>
 void* render_sm(bool strict, uint32_t mix, uint32_t v) {
-    if (strict) return mix ? render_v<I, C, true, 1>(v) : render_v<I, C, true, 0>(v);
-    return mix ? render_v<I, C, false, 1>(v) : render_v<I, C, false, 0>(v);
+    return strict ? render_m<I, C, true>(mix, v) : render_m<I, C, false>(mix, v);
 }
 
 // The render instantiation for [interp][chan][strict][mix][voices per lane].
@@ -103,72 +162,7 @@ __attribute__((visibility("hidden"))) int set_last_error(int code, const std::st
 }
 }  // namespace kc
 
-struct kc_synth {
-    kc_config cfg{};
-    int device = 0;
-    int sms = 148;
-    cudaStream_t stream = nullptr;
 
-    uint32_t cap = 0;           // pool slots, padded to 32
-    uint32_t tiles = 0;         // gate tiles per block
-    uint32_t params_per = 0;    // entries per params variant
-    uint32_t n_slots = 0;       // params variant slots
-    uint64_t pcm_len = 0;
-    uint32_t n_regions = 0, max_sample_len = 0;
-    SortLayout sort{};
-
-    // device buffers
-    uint32_t* pool[2] = {nullptr, nullptr};
-    int parity = 0;
-    int16_t* pcm = nullptr;
-    kc_region_params* params = nullptr;
-    uint32_t* gates = nullptr;
-    uint32_t* chan = nullptr;
-    kc_spawn_cmd* cmds = nullptr;
-    uint32_t cmds_cap = 0;
-    float* out = nullptr;
-    float* partial = nullptr;
-    float* partial_c = nullptr;
-    DevState* st = nullptr;
-    BlockCtl* ctl = nullptr;
-    uint32_t* sel_hist = nullptr;
-    uint32_t* counts = nullptr;
-    uint32_t* total = nullptr;
-    uint32_t* keys[2] = {nullptr, nullptr};
-    uint32_t* idx[2] = {nullptr, nullptr};
-
-    // launch geometry
-    uint32_t render_ctas = 0, render_warps = 0;
-    uint32_t vpl = 1;           // render voices per lane
-    size_t render_smem = 0;
-    uint32_t pool_ctas = 0;     // grid-stride passes
-    uint32_t compact_ctas = 0;  // chunked passes (compaction, sort)
-
-    // pinned host staging
-    uint32_t* h_gates = nullptr;
-    uint32_t* h_chan = nullptr;
-    kc_spawn_cmd* h_cmds = nullptr;
-    uint32_t h_cmds_cap = 0;
-    float* h_out = nullptr;
-    DevState* h_st = nullptr;
-
-    uint32_t want = 0;
-    bool bend = false, gain = false, variant = false;
-
-    // host mirror of BlockStats
-    kc_block_stats stats{};
-
-    bool profile = false;
-    cudaEvent_t ev[N_TIMERS + 1] = {};
-    double last_ms[N_TIMERS] = {};
-    bool have_timings = false;
-    // Profiling over many blocks in flight: one event set per enqueued block,
-    // read back at the next synchronisation.
-    std::vector<std::vector<cudaEvent_t>> ring;
-    size_t ring_pending = 0;
-    double total_ms[N_TIMERS] = {};
-    uint64_t total_blocks = 0;
-};
 
 namespace {
 
@@ -219,7 +213,7 @@ int validate(const kc_config& c) {
     if (c.max_steal_percent == 0 || c.max_steal_percent > 100)
         return fail(KC_ERR_INVALID, "max_steal_percent must be in 1..=100");
     if (c.steal_rule > 2 || c.admit_rule > 1 || c.interpolation > 2 || c.decay_curve > 1 ||
-        c.release_curve > 1 || c.mix_mode > 1)
+        c.release_curve > 1 || c.mix_mode > 2)
         return fail(KC_ERR_INVALID, "unknown enum value in config");
     if (c.voices_per_lane > 2) return fail(KC_ERR_INVALID, "voices_per_lane must be 0, 1 or 2");
     if (c.max_param_variants == 0 || c.max_param_variants > 64)
@@ -252,7 +246,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     cudaEvent_t* ev = s->ev;
     if (s->profile) {
         if (s->ring_pending == s->ring.size()) {
-            std::vector<cudaEvent_t> set(N_TIMERS + 1);
+            std::vector<cudaEvent_t> set(kc::N_TIMERS + 1);
             for (auto& e : set) KC_CUDA(cudaEventCreate(&e));
             s->ring.push_back(std::move(set));
         }
@@ -300,9 +294,11 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     // ---- 4. reduce ----
     const uint32_t samples = c.block_frames * 2;
     if (c.mix_mode == KC_MIX_F32_TREE)
-        k_reduce<0><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
+        k_reduce<KC_MIX_F32_TREE><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
+    else if (c.mix_mode == KC_MIX_TWO_SUM)
+        k_reduce<KC_MIX_TWO_SUM><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
     else
-        k_reduce<1><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
+        k_reduce<KC_MIX_F64><<<(samples + 31) / 32, 256, 0, q>>>(s->partial, s->partial_c, d_out, s->st, samples);
     if (s->profile) cudaEventRecord(ev[4], q);
     // ---- 5. compact (and sort) ----
     k_compact_count<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
@@ -336,7 +332,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
 // totals and keep the last block's as `last_ms`.
 void drain_timings(kc_synth* s) {
     for (size_t b = 0; b < s->ring_pending; ++b) {
-        for (int i = 0; i < N_TIMERS; ++i) {
+        for (int i = 0; i < kc::N_TIMERS; ++i) {
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, s->ring[b][i], s->ring[b][i + 1]);
             s->total_ms[i] += ms;
@@ -356,6 +352,40 @@ uint32_t launches_per_block(const kc_synth* s) {
     if (!s->cfg.sort_voices) n += 1;
     else n += 3 * ((s->sort.bits + 7) / 8) + 1;
     return n;
+}
+
+// Device bytes a context holds, from its geometry (kc_synth_create's
+// allocations, in the same order).
+uint64_t footprint(const kc_config& c, uint64_t cap, uint64_t pcm_len, uint64_t params_per, uint32_t n_slots,
+                   uint32_t tiles, uint32_t cmds_cap, uint32_t partial_slices, uint32_t compact_ctas) {
+    const uint64_t samples = (uint64_t)c.block_frames * 2;
+    uint64_t n = 2ull * VOICE_FIELDS * cap * 4;                                 // pool, double-buffered
+    n += std::max<uint64_t>(pcm_len, 1) * 2 + 64;                               // sample pool
+    n += params_per * sizeof(kc_region_params) * n_slots;                       // params variants
+    n += (uint64_t)tiles * (KC_GATE_SLOTS + KC_BEND_CHANNELS * KC_CHAN_FIELDS) * 4;
+    n += (uint64_t)cmds_cap * sizeof(kc_spawn_cmd) + samples * 4;               // spawn buffer, block
+    n += (uint64_t)partial_slices * samples * (c.mix_mode == KC_MIX_F64 ? 8 : 4);
+    if (c.mix_mode == KC_MIX_TWO_SUM) n += (uint64_t)partial_slices * samples * 4;
+    n += sizeof(DevState) + sizeof(BlockCtl) + SEL_ROUNDS * 256 * 4 + 256ull * compact_ctas * 4 + 16;
+    if (c.sort_voices) n += 4ull * cap * 4;                                     // keys, indices
+    return n;
+}
+
+uint32_t partial_slices_of(uint64_t cap, uint32_t vpl, uint32_t render_warps) {
+    const uint64_t batches = (cap + 32ull * vpl - 1) / (32ull * vpl);
+    return (uint32_t)std::min<uint64_t>(render_warps, std::max<uint64_t>(batches, 1));
+}
+
+// Render CTAs per SM for a config (the occupancy the grid is sized by).
+int render_occupancy(const kc_config& c, uint32_t vpl, size_t smem, int* per_sm) {
+    void* fn = render_table(c.interpolation, true, c.strict_fp != 0, c.mix_mode, vpl);
+    for (int ch = 0; ch < 2; ++ch) {
+        void* f2 = render_table(c.interpolation, ch != 0, c.strict_fp != 0, c.mix_mode, vpl);
+        KC_CUDA(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    KC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, RENDER_WARPS * 32, smem));
+    *per_sm = std::max(*per_sm, 1);
+    return KC_OK;
 }
 
 }  // namespace
@@ -436,15 +466,8 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     // Launch geometry: the render grid is every resident CTA of the device,
     // and the partial buffer has one slice per render warp.
     s->render_smem = (size_t)RENDER_WARPS * SM_WARP * sizeof(float);
-    void* fn = render_table(cfg->interpolation, true, cfg->strict_fp != 0, cfg->mix_mode, s->vpl);
-    KC_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->render_smem));
-    for (int ch = 0; ch < 2; ++ch) {
-        void* f2 = render_table(cfg->interpolation, ch != 0, cfg->strict_fp != 0, cfg->mix_mode, s->vpl);
-        KC_TRY(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->render_smem));
-    }
     int per_sm = 0;
-    KC_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, RENDER_WARPS * 32, s->render_smem));
-    per_sm = std::max(per_sm, 1);
+    if (int rc = render_occupancy(*cfg, s->vpl, s->render_smem, &per_sm)) return bail(rc);
     s->render_ctas = (uint32_t)(s->sms * per_sm);
     s->render_warps = s->render_ctas * RENDER_WARPS;
     s->pool_ctas = (uint32_t)s->sms * 4;
@@ -471,8 +494,14 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMalloc(&s->cmds, (size_t)s->cmds_cap * sizeof(kc_spawn_cmd)));
     const size_t samples = (size_t)cfg->block_frames * 2;
     KC_TRY(cudaMalloc(&s->out, samples * 4));
-    KC_TRY(cudaMalloc(&s->partial, (size_t)s->render_warps * samples * 4));
-    if (cfg->mix_mode != KC_MIX_F32_TREE) KC_TRY(cudaMalloc(&s->partial_c, (size_t)s->render_warps * samples * 4));
+    // One partial slice per render warp that can own a voice: at most one
+    // batch of 32 * voices-per-lane voices per slice, and never more slices
+    // than the grid has warps (live + admitted <= cap).
+    s->partial_slices = partial_slices_of(s->cap, s->vpl, s->render_warps);
+    const size_t slice_bytes = cfg->mix_mode == KC_MIX_F64 ? 8 : 4;
+    KC_TRY(cudaMalloc(&s->partial, (size_t)s->partial_slices * samples * slice_bytes));
+    if (cfg->mix_mode == KC_MIX_TWO_SUM)
+        KC_TRY(cudaMalloc(&s->partial_c, (size_t)s->partial_slices * samples * 4));
     KC_TRY(cudaMalloc(&s->st, sizeof(DevState)));
     KC_TRY(cudaMemset(s->st, 0, sizeof(DevState)));
     KC_TRY(cudaMalloc(&s->ctl, sizeof(BlockCtl)));
@@ -659,7 +688,7 @@ int kc_set_profile(kc_synth* s, int on) {
 
 int kc_timings_total(kc_synth* s, double* ms, size_t cap, uint64_t* blocks) {
     if (!s || !blocks) return fail(KC_ERR_INVALID, "null argument");
-    for (size_t i = 0; i < std::min<size_t>(cap, N_TIMERS); ++i) ms[i] = s->total_ms[i];
+    for (size_t i = 0; i < std::min<size_t>(cap, kc::N_TIMERS); ++i) ms[i] = s->total_ms[i];
     *blocks = s->total_blocks;
     return KC_OK;
 }
@@ -668,7 +697,7 @@ int kc_timings(kc_synth* s, const char** names, double* ms, size_t cap, size_t* 
     if (!s || !n) return fail(KC_ERR_INVALID, "null argument");
     *n = 0;
     if (!s->have_timings) return KC_OK;
-    const size_t k = std::min<size_t>(cap, N_TIMERS);
+    const size_t k = std::min<size_t>(cap, kc::N_TIMERS);
     for (size_t i = 0; i < k; ++i) {
         if (names) names[i] = kPassNames[i];
         if (ms) ms[i] = s->last_ms[i];
@@ -704,6 +733,47 @@ void* kc_stream(kc_synth* s) { return s ? (void*)s->stream : nullptr; }
 int kc_block_launches(kc_synth* s, uint32_t* out) {
     if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
     *out = launches_per_block(s);
+    return KC_OK;
+}
+
+int kc_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes) {
+    if (!free_bytes || !total_bytes) return fail(KC_ERR_INVALID, "null argument");
+    size_t f = 0, t = 0;
+    KC_CUDA(cudaSetDevice(device));
+    KC_CUDA(cudaMemGetInfo(&f, &t));
+    *free_bytes = f;
+    *total_bytes = t;
+    return KC_OK;
+}
+
+int kc_last_block_voices(kc_synth* s, uint32_t* rendered) {
+    if (!s || !rendered) return fail(KC_ERR_INVALID, "null argument");
+    *rendered = s->h_st->live_render;
+    return KC_OK;
+}
+
+uint64_t kc_synth_device_bytes(const kc_synth* s) {
+    if (!s) return 0;
+    return footprint(s->cfg, s->cap, s->pcm_len, s->params_per, s->n_slots, s->tiles, s->cmds_cap,
+                     s->partial_slices, s->compact_ctas);
+}
+
+int kc_estimate_device_bytes(const kc_config* cfg, uint64_t pool_len, uint32_t params_len, uint64_t* bytes) {
+    if (!cfg || !bytes) return fail(KC_ERR_INVALID, "null argument");
+    *bytes = 0;
+    if (int rc = validate(*cfg)) return rc;
+    const uint64_t slots = kc_pool_slots(cfg);
+    if (slots > 0x7FFFFFE0ull) return fail(KC_ERR_INVALID, "pool slots exceed 2^31");
+    int sms = 0, per_sm = 0;
+    KC_CUDA(cudaSetDevice((int)cfg->device));
+    KC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, (int)cfg->device));
+    const uint32_t vpl = cfg->voices_per_lane == 2 ? 2u : 1u;
+    if (int rc = render_occupancy(*cfg, vpl, (size_t)RENDER_WARPS * SM_WARP * sizeof(float), &per_sm)) return rc;
+    const uint64_t cap = (slots + 31) & ~31ull;
+    const uint32_t render_warps = (uint32_t)(sms * per_sm) * RENDER_WARPS;
+    *bytes = footprint(*cfg, cap, pool_len, params_len, cfg->max_param_variants,
+                       cfg->block_frames / cfg->gate_frames, 4096, partial_slices_of(cap, vpl, render_warps),
+                       (uint32_t)sms * 2);
     return KC_OK;
 }
 

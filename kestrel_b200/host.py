@@ -61,6 +61,7 @@ HOST_SYMBOLS = {
     "kh_bank_presets": (C.c_uint32, [_P]),
     "kh_bank_max_sample_len": (C.c_uint32, [_P]),
     "kh_bank_pool_rate": (C.c_uint32, [_P]),
+    "kh_bank_filter_inputs": (C.c_int, [_P, _P, _P, _P, C.c_uint32]),
     "kh_midi_spec_default": (None, [C.POINTER(KhMidiSpec)]),
     "kh_driver_open": (_P, [C.POINTER(N.KcConfig), C.POINTER(KhOptions), _P, C.POINTER(KhMidiSpec)]),
     "kh_driver_destroy": (None, [_P]),
@@ -221,6 +222,16 @@ class Bank:
         self.presets = self._lib.kh_bank_presets(h)
         self.max_sample_len = self._lib.kh_bank_max_sample_len(h)
         self.pool_rate = self._lib.kh_bank_pool_rate(h)
+
+    def filter_inputs(self):
+        """(cutoff Hz, Q cB, on) per variant-0 params entry."""
+        n = self.params.size
+        fc = np.empty(n, np.float32)
+        q = np.empty(n, np.float32)
+        on = np.empty(n, np.uint8)
+        if self._lib.kh_bank_filter_inputs(self._h, N.ptr(fc), N.ptr(q), N.ptr(on), n) != 0:
+            raise RuntimeError(self._lib.kh_last_error().decode())
+        return fc, q, on.astype(bool)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -20,7 +20,7 @@ INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC = 0, 1, 2
 CURVE_EXPONENTIAL, CURVE_LINEAR = 0, 1
 STEAL_OLDEST, STEAL_DROP_NEW, STEAL_QUIETEST = 0, 1, 2
 ADMIT_LOUDEST, ADMIT_EVEN = 0, 1
-MIX_F32_TREE, MIX_TWO_SUM = 0, 1
+MIX_F32_TREE, MIX_TWO_SUM, MIX_F64 = 0, 1, 2
 
 ENV_ATTACK, ENV_DECAY, ENV_SUSTAIN, ENV_RELEASE, ENV_DEAD = 0, 1, 2, 3, 4
 GATE_SLOTS = 2048
@@ -94,6 +94,27 @@ def default_config(**overrides) -> KcConfig:
     return c
 
 
+class KcBatchConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_uint32), ("max_jobs", C.c_uint32), ("block_frames", C.c_uint32),
+        ("interpolation", C.c_uint32), ("strict_fp", C.c_uint32), ("mix_mode", C.c_uint32),
+        ("voices_per_lane", C.c_uint32), ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+
+
+def batch_config_for(cfg: KcConfig, max_jobs: int = 256, use_graph: bool = True) -> KcBatchConfig:
+    """The batch variant that accepts contexts created with `cfg`."""
+    b = KcBatchConfig()
+    b.device = cfg.device
+    b.max_jobs = max_jobs
+    b.block_frames = cfg.block_frames
+    b.interpolation = cfg.interpolation
+    b.strict_fp = cfg.strict_fp
+    b.mix_mode = cfg.mix_mode
+    b.voices_per_lane = 2 if cfg.voices_per_lane == 2 else 1
+    b.use_graph = 1 if use_graph else 0
+    return b
+
+
 # Every symbol include/kestrel_cuda.h declares, with its ctypes signature.
 _P = C.c_void_p
 CUDA_SYMBOLS = {
@@ -120,6 +141,16 @@ CUDA_SYMBOLS = {
     "kc_stream": (_P, [_P]),
     "kc_block_launches": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "kc_read_pool": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_uint32)]),
+    "kc_design_lowpass_f64": (C.c_int, [_P, _P, C.c_uint32, C.c_float, _P, C.c_int]),
+    "kc_batch_config_default": (C.c_int, [C.POINTER(KcBatchConfig)]),
+    "kc_batch_create": (C.c_int, [C.POINTER(KcBatchConfig), C.POINTER(_P)]),
+    "kc_batch_destroy": (None, [_P]),
+    "kc_batch_render": (C.c_int, [_P, C.POINTER(_P), C.c_uint32, C.POINTER(_P)]),
+    "kc_batch_last_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "kc_synth_device_bytes": (C.c_uint64, [_P]),
+    "kc_estimate_device_bytes": (C.c_int, [C.POINTER(KcConfig), C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "kc_last_block_voices": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
+    "kc_device_memory": (C.c_int, [C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "kc_render_block_noalloc": (C.c_int, [C.POINTER(KcConfig), _P, C.c_uint32, C.c_uint32, _P, C.c_uint64, _P,
                                           C.c_uint32, C.c_uint32, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
 }

@@ -128,3 +128,41 @@ def test_rerun_byte_identical():
         outs.append(np.concatenate(o))
         cu.close()
     assert outs[0].tobytes() == outs[1].tobytes()
+
+
+@gpu
+def test_f64_mix_matches_the_oracle_f64_mix():
+    """KC_MIX_F64 accumulates the same f32 voice terms in double, like the
+    oracle's f64 mixdown (src/cpu.rs:589-590): the blocks agree to within one
+    f32 ulp (only the f64 summation order differs)."""
+    sc = make_scenario(seed=13, mix_mode=N.MIX_F64)
+    cu, orc = _pair(sc)
+    o_c, _, _, _ = run(cu, sc)
+    o_o, _, _, _ = run(orc, sc)
+    for b in range(len(sc.blocks)):
+        ulp = np.spacing(np.abs(o_o[b]).astype(np.float32))
+        assert np.all(np.abs(o_c[b].astype(np.float64) - o_o[b]) <= ulp), f"block {b}"
+
+
+@gpu
+def test_fp64_lowpass_design():
+    """kc_design_lowpass_f64 returns the exact RBJ design rounded once to f32.
+    The reference's f32 design agrees with it within the cancellation bound of
+    (1 - cos w0) in f32: a few ulp(1) / (1 - cos w0), relative, on b0 and b1
+    (about 1e-5 at 1 kHz, 50x that at 20 Hz)."""
+    from kestrel_b200 import host as H
+    from kestrel_b200.precision import _design_exact
+    lib = N.cuda_lib()
+    fc = np.array([20.0, 35.0, 80.0, 200.0, 1000.0, 8000.0], np.float32)
+    q_cb = np.array([290.0, 150.0, 30.0, 0.0, 30.0, 30.0], np.float32)
+    out = np.empty((fc.size, 4), np.float32)
+    N.check(lib.kc_design_lowpass_f64(N.ptr(fc), N.ptr(q_cb), fc.size, 48000.0, N.ptr(out), 0), lib)
+    exact = _design_exact(fc.astype(np.float64), q_cb.astype(np.float64), 48000.0)
+    rel = np.abs(out.astype(np.float64) - exact) / np.abs(exact)
+    assert np.all(rel <= 2.0 ** -23), rel
+    for i in (4, 5):
+        ref = np.array(H.biquad_lowpass(float(fc[i]), float(q_cb[i]), 48000.0), np.float64)
+        omc = 1.0 - np.cos(2 * np.pi * float(fc[i]) / 48000.0)
+        bound = 4 * 2.0 ** -24 / omc
+        assert np.all(np.abs(ref[:2] - out[i, :2]) / np.abs(out[i, :2]) <= bound), (i, ref, out[i])
+        assert np.all(np.abs(ref[2:] - out[i, 2:]) <= 8 * np.spacing(np.abs(out[i, 2:]))), (i, ref, out[i])
