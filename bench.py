@@ -59,7 +59,11 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--workload", choices=["steal", "black", "plain"], default="steal")
+    ap.add_argument("--workload", choices=["steal", "black", "plain", "served"], default="steal")
+    ap.add_argument("--served-jobs", type=int, default=32, help="jobs of the served workload")
+    ap.add_argument("--served-seconds", type=float, default=2.0,
+                    help="audio seconds rendered per served job (its MIDI keeps its full length)")
+    ap.add_argument("--served-arrivals", choices=["poisson", "queued"], default="poisson")
     ap.add_argument("--preroll", type=int, default=None)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -299,6 +303,68 @@ def run_oracle(workload, seed, threads, max_blocks, max_seconds):
             "sample_rate": cfg.sample_rate}
 
 
+def run_served(args):
+    """The batched-and-served configuration: the same seeded job mix through
+    the render server twice -- continuous batching (one kc_batch_render per
+    step for every resident job, graph-replayed) and the plain path (one job
+    at a time through kc_render) -- end to end through ks_serve, host driver
+    included. Returns one JSON line."""
+    import torch
+    from kestrel_b200 import serve as S
+
+    torch.cuda.set_device(0)
+    jobs = S.served_jobs(args.served_jobs, seed=args.seed, max_seconds=args.served_seconds)
+    queued = args.served_arrivals == "queued"
+    # warm-up: module load, graph capture paths, host pools
+    S.serve(S.served_jobs(3, seed=args.seed + 99, max_seconds=0.2, notes=(10_000, 20_000),
+                          pools=(16_384, 32_768)), mode=S.MODE_BATCHED, max_jobs=4, realtime_arrivals=False)
+    S.serve(S.served_jobs(1, seed=args.seed + 98, max_seconds=0.2, notes=(10_000, 20_000),
+                          pools=(16_384, 32_768)), mode=S.MODE_SEQUENTIAL, realtime_arrivals=False)
+    clocks = ClockSampler(0)
+    clocks.start()
+    bat = S.serve(jobs, mode=S.MODE_BATCHED, max_jobs=256, realtime_arrivals=not queued)
+    clk = clocks.stop()
+    seq = S.serve(jobs, mode=S.MODE_SEQUENTIAL, realtime_arrivals=not queued)
+
+    def summary(r):
+        lat = r.latencies()
+        vs = r.stats.voice_samples
+        return {"voice_samples_per_s": vs / r.stats.wall_s, "wall_s": r.stats.wall_s,
+                "gpu_s": r.stats.gpu_ms * 1e-3 if r.stats.gpu_ms else None,
+                "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                "mean_latency_s": float(lat.mean()), "steps": int(r.stats.steps),
+                "max_resident": int(r.stats.max_resident), "host_threads": int(r.stats.host_threads),
+                "peak_device_gb": r.stats.peak_device_bytes / 1e9, "voice_samples": int(vs),
+                "failed_jobs": sum(1 for j in r.jobs if j.status != 0)}
+
+    b, s = summary(bat), summary(seq)
+    same = bat.hashes() == seq.hashes()
+    audio_s = sum(j.blocks for j in bat.jobs) * 4096 / 48000
+    blocks = sum(j.blocks for j in bat.jobs)
+    line = {
+        "metric": "aggregate voice-samples/s of the served job mix (p50/p99 job latency beside)",
+        "value": b["voice_samples_per_s"], "unit": "voice-samples/s", "n_gpus": 1,
+        "steps": int(bat.stats.steps), "warmup": 1, "ms_per_step": b["wall_s"] * 1e3 / max(bat.stats.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "cuda-batched-served",
+        "config": {"workload": f"served: {len(jobs)} jobs, Poisson arrivals at 20 jobs/s"
+                               f"{' (all queued at start)' if queued else ''}, notes log-uniform 10k-20M, "
+                               f"durations U[5,300] s, pools log-uniform 16k-2M, 1-128 presets per job; "
+                               f"each job bounded to its first {args.served_seconds:g} s of audio",
+                   "jobs": len(jobs), "job_audio_s": audio_s, "job_blocks": blocks,
+                   "arrivals": "queued" if queued else "poisson-realtime"},
+        "batched": b, "sequential_plain_path": s,
+        "ratio_vs_plain_path": b["voice_samples_per_s"] / s["voice_samples_per_s"],
+        "p50_latency_s": b["p50_latency_s"], "p99_latency_s": b["p99_latency_s"],
+        "outputs_identical_to_plain_path": same,
+        "e2e": {"value": b["voice_samples_per_s"], "unit": "voice-samples/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": 32832, "note": "the served run is itself end to end: ks_serve with "
+                                                    "host drivers, host buffers and per-block readback"},
+        "clocks": clk,
+    }
+    return line
+
+
 def workload_desc(name):
     return {
         "steal": "steal-saturation: 200M notes / 120 s, log-normal durations (median 6 s, sigma 0.5), "
@@ -339,6 +405,11 @@ def main(argv=None):
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line), flush=True)
+        return 0
+
+    if args.workload == "served":
+        if rank == 0:
+            print(json.dumps(run_served(args)), flush=True)
         return 0
 
     if world > 1:

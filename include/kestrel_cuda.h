@@ -142,7 +142,9 @@ typedef struct kc_config {
     uint32_t strict_fp;          /* 1: no FMA contraction anywhere in the voice DSP */
     uint32_t device;             /* CUDA ordinal */
     uint32_t voices_per_lane;    /* render voices per GPU lane: 0 = default (1), 1 or 2 */
-    uint32_t reserved[6];
+    uint32_t sort_radix_bits;    /* key bits per pool-sort pass, 4..=10; 0 = default (8). The
+                                    sorted order is the same for every width. */
+    uint32_t reserved[5];
 } kc_config;
 
 typedef struct kc_synth kc_synth;
@@ -168,6 +170,12 @@ void kc_synth_destroy(kc_synth* s);
  * counterpart in the reference trait; it is how a render is checkpointed or
  * forked (the benchmark forks one to replay recorded blocks from HBM). */
 int kc_synth_clone(kc_synth* src, kc_synth** out);
+/* The same, with other tunables: `cfg` must equal the source's config except
+ * in voices_per_lane and sort_radix_bits, which change how a block is
+ * computed but not the voice state it leaves (voices per lane also changes
+ * the summation order of the mix, within its tolerance). The autotuner times
+ * its candidates on such clones of one pre-rolled context. */
+int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out);
 
 /* Backend::set_gates (src/backend.rs:23-25): tiles * KC_GATE_SLOTS words,
  * tile-major; tiles = block_frames / gate_frames. */
@@ -270,8 +278,9 @@ int kc_render_block_noalloc(const kc_config* cfg, uint32_t* d_pool, uint32_t cap
  * with kc_set_gates / kc_set_channels / kc_spawn, exactly as before kc_render;
  * a job's output block, state and stats are byte-identical to rendering that
  * context alone with kc_render. All jobs must match the batch's device,
- * block_frames, interpolation, strict_fp, mix_mode and voices_per_lane; the
- * steal and admit rules, pool sizes, banks and sort setting are per job. */
+ * block_frames, interpolation, strict_fp, mix_mode, voices_per_lane and
+ * sort_radix_bits; the steal and admit rules, pool sizes, banks and sort
+ * setting are per job. */
 typedef struct kc_batch_config {
     uint32_t device;
     uint32_t max_jobs;           /* 1..=1024 */
@@ -281,7 +290,8 @@ typedef struct kc_batch_config {
     uint32_t mix_mode;           /* KC_MIX_* */
     uint32_t voices_per_lane;    /* 0 or 1: one voice per lane; 2: two */
     uint32_t use_graph;          /* 1: replay a captured graph; 0: launch each pass */
-    uint32_t reserved[8];
+    uint32_t sort_radix_bits;    /* 0 = 8, else 4..=10, as kc_config */
+    uint32_t reserved[7];
 } kc_batch_config;
 
 typedef struct kc_batch kc_batch;
@@ -295,8 +305,10 @@ void kc_batch_destroy(kc_batch* b);
 int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* const* outs);
 /* Device milliseconds of the last kc_batch_render's launch sequence. */
 int kc_batch_last_ms(kc_batch* b, float* ms);
-/* Device memory a context holds, in bytes, and the same figure for a context
- * not yet created (the serving loop admits jobs by it). */
+/* Device memory a context holds now, in bytes, and the most a context not yet
+ * created can come to hold (its spawn buffer grown to one command per pool
+ * slot, the largest block admission can produce). The serving loop admits
+ * jobs by the second figure. */
 uint64_t kc_synth_device_bytes(const kc_synth* s);
 int kc_estimate_device_bytes(const kc_config* cfg, uint64_t pool_len, uint32_t params_len, uint64_t* bytes);
 /* Free and total memory of a device, in bytes. */

@@ -64,7 +64,10 @@ typedef struct ks_server_config {
     uint32_t realtime_arrivals;  /* 1: a job is visible at arrival_s on the wall clock; 0: all at start */
     ks_block_fn on_block;        /* optional */
     void* user;
-    uint32_t reserved[8];
+    uint32_t autotune;           /* 1: before serving, run ks_autotune (voices per lane, sort digit
+                                    width) on the job with the largest voice pool and give every
+                                    job the winner */
+    uint32_t reserved[7];
 } ks_server_config;
 
 typedef struct ks_job_result {
@@ -93,7 +96,45 @@ typedef struct ks_run_stats {
     uint64_t peak_device_bytes;  /* largest admitted total */
     uint32_t max_resident;
     uint32_t host_threads;
+    uint32_t tuned_voices_per_lane;  /* the autotuner's choice (0: not tuned) */
+    uint32_t tuned_sort_radix_bits;
+    double tune_s;                   /* wall seconds the autotuner took (not in wall_s) */
 } ks_run_stats;
+
+/* ---- autotuner ------------------------------------------------------------
+ * Picks voices per lane, pool-sort digit width and (when allowed) block
+ * length for a job. For each block length it renders the job's first
+ * preroll_blocks blocks, snapshots the context, records the next timed_blocks
+ * blocks' inputs, then replays them on a clone of the snapshot for every
+ * (voices per lane, digit width) candidate (kc_synth_clone_config) and times
+ * the replays on the device. The fastest candidate by voice-samples per
+ * device second wins. Voices per lane and digit width never change the voice
+ * state a block leaves; block length changes when blocks are admitted and is
+ * tried only when the caller lists lengths. */
+typedef struct ks_tune_space {
+    uint32_t voices_per_lane_mask; /* bit v-1: try v voices per lane (v = 1, 2); 0 = both */
+    uint32_t radix_mask;           /* bit r: try r-bit sort digits (4..10); 0 = {6, 8, 10} */
+    uint32_t block_frames[4];      /* lengths to try (0 = unused); all 0 = the job's own */
+    uint32_t preroll_blocks;       /* untimed blocks before the snapshot; 0 = 16 */
+    uint32_t timed_blocks;         /* replayed and timed per candidate; 0 = 4 */
+    uint32_t reserved[6];
+} ks_tune_space;
+
+typedef struct ks_tune_result {
+    uint32_t voices_per_lane;
+    uint32_t sort_radix_bits;
+    uint32_t block_frames;
+    uint32_t blocks;               /* blocks timed */
+    double device_ms;              /* summed pass time of the timed blocks */
+    uint64_t voice_samples;        /* voices rendered x block_frames over them */
+    double voice_samples_per_s;
+} ks_tune_result;
+
+/* `best` receives the job's config with the winning tunables. `results`
+ * (capacity `cap`, may be NULL) receives every candidate's timing; *n the
+ * number of candidates. */
+int ks_autotune(const ks_job_spec* job, const ks_tune_space* space, kc_config* best, ks_tune_result* results,
+                uint32_t cap, uint32_t* n);
 
 void ks_server_config_default(ks_server_config* c);
 /* Runs every job to completion. `results` holds n_jobs entries (in the order

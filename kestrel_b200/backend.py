@@ -45,13 +45,18 @@ class CudaSynth:
         self.tiles = cfg.block_frames // cfg.gate_frames
         self.params_per = params.size
 
-    def clone(self) -> "CudaSynth":
-        """A second context in this one's exact state (kc_synth_clone)."""
+    def clone(self, cfg: N.KcConfig | None = None) -> "CudaSynth":
+        """A second context in this one's exact state (kc_synth_clone), or
+        with other tunables -- voices_per_lane, sort_radix_bits -- when `cfg`
+        is given (kc_synth_clone_config)."""
         h = C.c_void_p()
-        N.check(self._lib.kc_synth_clone(self._h, C.byref(h)), self._lib)
+        if cfg is None:
+            N.check(self._lib.kc_synth_clone(self._h, C.byref(h)), self._lib)
+        else:
+            N.check(self._lib.kc_synth_clone_config(self._h, C.byref(cfg), C.byref(h)), self._lib)
         other = object.__new__(CudaSynth)
         other._lib = self._lib
-        other.cfg = self.cfg
+        other.cfg = cfg if cfg is not None else self.cfg
         other._h = h
         other.block_frames = self.block_frames
         other.tiles = self.tiles

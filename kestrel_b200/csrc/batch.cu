@@ -39,7 +39,6 @@ using namespace kc;
 namespace {
 
 constexpr uint32_t MAX_JOBS = 1024;       // one plan CTA scans them
-constexpr uint32_t SORT_PASSES_MAX = 4;   // 32-bit keys, 8-bit digits
 constexpr uint32_t SEL_CHUNK = 8192;      // voices per select / mark item
 constexpr uint32_t CMP_CHUNK = 4096;      // voices per compaction / sort item
 constexpr uint32_t GATHER_CHUNK = 2048;   // voices per gather item
@@ -300,34 +299,48 @@ __global__ void __launch_bounds__(256) kb_compact_scatter(const BatchHeader* hdr
 
 // Pass p reads keys[p & 1] (the pool on pass 0) and writes keys[(p + 1) & 1],
 // the alternation the single-context path uses.
+template <uint32_t RB>
 __global__ void __launch_bounds__(256) kb_sort_count(const BatchHeader* hdr, const JobDesc* jobs,
                                                      const BatchPlan* plan, uint32_t p) {
     for_items<K_SORT>(hdr, plan, [&](uint32_t j, uint32_t c, uint32_t m) {
         const JobDesc& d = jobs[j];
         if (p >= d.sort_passes) return;
-        sort_count_body(d.pa, d.sort, p ? d.keys[p & 1u] : nullptr, 8u * p, d.counts, c, m);
+        sort_count_body<RB>(d.pa, d.sort, p ? d.keys[p & 1u] : nullptr, RB * p, d.counts, c, m);
     });
 }
 
+template <uint32_t RB>
 __global__ void __launch_bounds__(1024) kb_sort_scan(const BatchHeader* hdr, const JobDesc* jobs,
                                                      const BatchPlan* plan, uint32_t p) {
     const uint32_t n = hdr->n_jobs;
     for (uint32_t j = blockIdx.x; j < n; j += gridDim.x) {
         const JobDesc& d = jobs[j];
-        if (p < d.sort_passes) scan_counts_body(d.counts, 256u * plan->cmp_ctas[j], d.total + 1);
+        if (p < d.sort_passes) scan_counts_body(d.counts, (1u << RB) * plan->cmp_ctas[j], d.total + 1);
         __syncthreads();
     }
 }
 
+template <uint32_t RB>
 __global__ void __launch_bounds__(256) kb_sort_scatter(const BatchHeader* hdr, const JobDesc* jobs,
                                                        const BatchPlan* plan, uint32_t p) {
     for_items<K_SORT>(hdr, plan, [&](uint32_t j, uint32_t c, uint32_t m) {
         const JobDesc& d = jobs[j];
         if (p >= d.sort_passes) return;
         const uint32_t cur = p & 1u;
-        sort_scatter_body(d.pa, d.sort, p ? d.keys[cur] : nullptr, p ? d.idx[cur] : nullptr, d.keys[cur ^ 1u],
-                          d.idx[cur ^ 1u], 8u * p, d.counts, c, m);
+        sort_scatter_body<RB>(d.pa, d.sort, p ? d.keys[cur] : nullptr, p ? d.idx[cur] : nullptr, d.keys[cur ^ 1u],
+                              d.idx[cur ^ 1u], RB * p, d.counts, c, m);
     });
+}
+
+// The batch's sort passes at its digit width: enough passes for a 32-bit key;
+// a job whose key is shorter skips the passes it does not need.
+template <uint32_t RB>
+void sort_passes(cudaStream_t q, uint32_t P, const BatchHeader* h, const JobDesc* J, const BatchPlan* pl) {
+    for (uint32_t p = 0; p < (32u + RB - 1u) / RB; ++p) {
+        kb_sort_count<RB><<<P, 256, 0, q>>>(h, J, pl, p);
+        kb_sort_scan<RB><<<P, 1024, 0, q>>>(h, J, pl, p);
+        kb_sort_scatter<RB><<<P, 256, 0, q>>>(h, J, pl, p);
+    }
 }
 
 __global__ void __launch_bounds__(256) kb_sort_gather(const BatchHeader* hdr, const JobDesc* jobs,
@@ -398,6 +411,7 @@ struct kc_batch {
     int sms = 148;
     cudaStream_t stream = nullptr;
     uint32_t vpl = 1;
+    uint32_t radix = 8;
     void* render_fn = nullptr;
     size_t render_smem = 0;
     uint32_t render_ctas = 0;
@@ -470,10 +484,14 @@ int enqueue_passes(kc_batch* b) {
     kb_compact_count<<<P, 256, 0, q>>>(h, J, pl);
     kb_scan_commit<<<P, 1024, 0, q>>>(h, J, pl);
     kb_compact_scatter<<<P, 256, 0, q>>>(h, J, pl);
-    for (uint32_t p = 0; p < SORT_PASSES_MAX; ++p) {
-        kb_sort_count<<<P, 256, 0, q>>>(h, J, pl, p);
-        kb_sort_scan<<<P, 1024, 0, q>>>(h, J, pl, p);
-        kb_sort_scatter<<<P, 256, 0, q>>>(h, J, pl, p);
+    switch (b->radix) {
+        case 4: sort_passes<4>(q, P, h, J, pl); break;
+        case 5: sort_passes<5>(q, P, h, J, pl); break;
+        case 6: sort_passes<6>(q, P, h, J, pl); break;
+        case 7: sort_passes<7>(q, P, h, J, pl); break;
+        case 9: sort_passes<9>(q, P, h, J, pl); break;
+        case 10: sort_passes<10>(q, P, h, J, pl); break;
+        default: sort_passes<8>(q, P, h, J, pl); break;
     }
     kb_sort_gather<<<P, 256, 0, q>>>(h, J, pl);
     kb_collect<<<P, 256, 0, q>>>(h, J);
@@ -484,7 +502,7 @@ int enqueue_passes(kc_batch* b) {
 bool same_variant(const kc_batch* b, const kc_synth* s) {
     return s->device == b->device && s->cfg.block_frames == b->cfg.block_frames &&
            s->cfg.interpolation == b->cfg.interpolation && (s->cfg.strict_fp != 0) == (b->cfg.strict_fp != 0) &&
-           s->cfg.mix_mode == b->cfg.mix_mode && s->vpl == b->vpl;
+           s->cfg.mix_mode == b->cfg.mix_mode && s->vpl == b->vpl && s->radix == b->radix;
 }
 
 }  // namespace
@@ -514,10 +532,13 @@ int kc_batch_create(const kc_batch_config* cfg, kc_batch** out) {
         return fail(KC_ERR_INVALID, "block_frames must be a non-zero multiple of 16, at most 65535");
     if (cfg->interpolation > 2 || cfg->mix_mode > 2 || cfg->voices_per_lane > 2)
         return fail(KC_ERR_INVALID, "unknown enum value in batch config");
+    if (cfg->sort_radix_bits && (cfg->sort_radix_bits < SORT_RADIX_MIN || cfg->sort_radix_bits > SORT_RADIX_MAX))
+        return fail(KC_ERR_INVALID, "sort_radix_bits must be 0 or in 4..=10");
     kc_batch* b = new kc_batch();
     b->cfg = *cfg;
     b->device = (int)cfg->device;
     b->vpl = cfg->voices_per_lane == 2 ? 2u : 1u;
+    b->radix = cfg->sort_radix_bits ? cfg->sort_radix_bits : SORT_RADIX_DEFAULT;
     auto bail = [&](int rc) {
         free_batch(b);
         delete b;
@@ -594,7 +615,7 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         if (!same_variant(b, s))
             return fail(KC_ERR_INVALID, "job " + std::to_string(j) +
                                             " differs from the batch in device, block_frames, interpolation, "
-                                            "strict_fp, mix_mode or voices_per_lane");
+                                            "strict_fp, mix_mode, voices_per_lane or sort_radix_bits");
     }
     cudaSetDevice(b->device);
     cudaStream_t q = b->stream;
@@ -644,6 +665,7 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         ra.pool = pa.pool;
         ra.cap = s->cap;
         ra.pcm = s->pcm;
+        ra.pcmf = s->pcmf;
         ra.pcm_len = (uint32_t)std::min<uint64_t>(s->pcm_len, 0xFFFFFFFFull);
         ra.params = s->params;
         ra.params_per = s->params_per;
@@ -676,7 +698,7 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         d.want = s->want;
         d.chan_active = (s->bend ? 1u : 0u) | (s->gain ? 2u : 0u) | (s->variant ? 4u : 0u);
         d.samples = c.block_frames * 2;
-        d.sort_passes = c.sort_voices ? (s->sort.bits + 7) / 8 : 0u;
+        d.sort_passes = c.sort_voices ? (s->sort.bits + s->radix - 1) / s->radix : 0u;
         d.sel_cap = s->pool_ctas;
         d.cmp_cap = s->compact_ctas;
     }

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kc::RENDER_WARPS * 32, 3) k_noalloc_render(kc:
     float* sm = reinterpret_cast<float*>(smem4) + (threadIdx.x >> 5) * kc::SM_WARP;
     const uint32_t gw = blockIdx.x * kc::RENDER_WARPS + (threadIdx.x >> 5);
     const uint32_t tw = gridDim.x * kc::RENDER_WARPS;
-    kc::render_batches<INTERP, CHAN, STRICT, MIX, 1>(a, sm, gw, tw, a.st->live_render);
+    kc::render_batches<INTERP, CHAN, STRICT, MIX, 1, false>(a, sm, gw, tw, a.st->live_render);
 }
 
 // Fold the slices into the block in a fixed order (eight warps each sum a
@@ -240,7 +240,7 @@ int kc_render_block_noalloc(const kc_config* cfg, uint32_t* d_pool, uint32_t cap
         void* fn = render_pick(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode);
         void* args[] = {&ra};
         const unsigned ctas = (nbatch + kc::RENDER_WARPS - 1) / kc::RENDER_WARPS;
-        // 8 warp tiles of 32 x 36 floats = 36,864 bytes: under the 48 KiB
+        // 8 warp tiles of 16 x 72 floats = 36,864 bytes: under the 48 KiB
         // every kernel may take without an opt-in attribute.
         const size_t smem = (size_t)kc::RENDER_WARPS * kc::SM_WARP * sizeof(float);
         cudaError_t e = cudaLaunchKernel(fn, dim3(ctas), dim3(kc::RENDER_WARPS * 32), args, smem, q);

@@ -350,47 +350,58 @@ __device__ __forceinline__ uint32_t sort_chunk(uint32_t n, uint32_t nblocks) {
     return (c + 255u) & ~255u;
 }
 
+// Digit widths the pool sort can run with (kc_config::sort_radix_bits): a
+// pass handles RB key bits with 2^RB bins per CTA.
+constexpr uint32_t SORT_RADIX_MIN = 4, SORT_RADIX_MAX = 10, SORT_RADIX_DEFAULT = 8;
+
 // Pass `shift`: count digit occurrences per CTA chunk into counts[d * G + cta].
 // Pass 0 computes keys from the pool; later passes read the key array.
+template <uint32_t RB>
 __device__ __forceinline__ void sort_count_body(PoolArgs a, SortLayout L, const uint32_t* keys, uint32_t shift,
                                                 uint32_t* counts, uint32_t cta, uint32_t ctas) {
-    __shared__ uint32_t h[256];
+    constexpr uint32_t BINS = 1u << RB;
+    __shared__ uint32_t h[BINS];
     const uint32_t n = a.st->live_render;
-    h[threadIdx.x] = 0u;
+    for (uint32_t d = threadIdx.x; d < BINS; d += blockDim.x) h[d] = 0u;
     __syncthreads();
     const uint32_t chunk = sort_chunk(n, ctas);
     const uint32_t lo = cta * chunk, hi = min(n, lo + chunk);
     for (uint32_t i = lo + threadIdx.x; i < hi; i += 256u) {
         const uint32_t k = keys ? keys[i] : sort_key(a.pool, a.cap, i, L);
-        atomicAdd(&h[(k >> shift) & 255u], 1u);
+        atomicAdd(&h[(k >> shift) & (BINS - 1u)], 1u);
     }
     __syncthreads();
-    counts[threadIdx.x * ctas + cta] = h[threadIdx.x];
+    for (uint32_t d = threadIdx.x; d < BINS; d += blockDim.x) counts[d * ctas + cta] = h[d];
 }
 
 // Stable scatter of one pass. keys_in == nullptr on the first pass (keys and
-// indices come from the pool order).
+// indices come from the pool order). Each 256-key step ranks equal digits
+// inside a warp with __match_any_sync and across the CTA's 8 warps with
+// per-warp digit counts, so keys keep their input order within a digit.
+template <uint32_t RB>
 __device__ __forceinline__ void sort_scatter_body(PoolArgs a, SortLayout L, const uint32_t* keys_in,
                                                       const uint32_t* idx_in, uint32_t* keys_out,
                                                       uint32_t* idx_out, uint32_t shift,
                                                       const uint32_t* offsets, uint32_t cta, uint32_t ctas) {
-    __shared__ uint32_t run[256];
-    __shared__ uint32_t wcnt[8][256];
+    constexpr uint32_t BINS = 1u << RB;
+    __shared__ uint32_t run[BINS];
+    __shared__ uint32_t wcnt[8][BINS];
     const uint32_t n = a.st->live_render;
     const uint32_t lane = lane_id(), w = threadIdx.x >> 5;
-    run[threadIdx.x] = offsets[threadIdx.x * ctas + cta];
+    for (uint32_t d = threadIdx.x; d < BINS; d += blockDim.x) run[d] = offsets[d * ctas + cta];
     const uint32_t chunk = sort_chunk(n, ctas);
     const uint32_t lo = cta * chunk, hi = min(n, lo + chunk);
     for (uint32_t t0 = lo; t0 < hi; t0 += 256u) {
-        for (uint32_t k = 0; k < 8; ++k) wcnt[k][threadIdx.x] = 0u;
+        for (uint32_t d = threadIdx.x; d < BINS; d += blockDim.x)
+            for (uint32_t k = 0; k < 8; ++k) wcnt[k][d] = 0u;
         __syncthreads();
         const uint32_t i = t0 + threadIdx.x;
         const bool valid = i < hi;
-        uint32_t key = 0, id = 0, d = 256u + lane;  // invalid lanes get unique dummy digits
+        uint32_t key = 0, id = 0, d = BINS + lane;  // invalid lanes get unique dummy digits
         if (valid) {
             key = keys_in ? keys_in[i] : sort_key(a.pool, a.cap, i, L);
             id = idx_in ? idx_in[i] : i;
-            d = (key >> shift) & 255u;
+            d = (key >> shift) & (BINS - 1u);
         }
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
         const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
@@ -404,14 +415,16 @@ __device__ __forceinline__ void sort_scatter_body(PoolArgs a, SortLayout L, cons
             idx_out[dst] = id;
         }
         __syncthreads();
-        uint32_t tot = 0;
-        for (uint32_t k = 0; k < 8; ++k) tot += wcnt[k][threadIdx.x];
-        run[threadIdx.x] += tot;
+        for (uint32_t dd = threadIdx.x; dd < BINS; dd += blockDim.x) {
+            uint32_t tot = 0;
+            for (uint32_t k = 0; k < 8; ++k) tot += wcnt[k][dd];
+            run[dd] += tot;
+        }
         __syncthreads();
     }
 }
 
-// Scan counts[256 * G] digit-major (one CTA).
+// Scan counts[2^RB * G] digit-major (one CTA).
 // (k_scan_counts handles it: it is a plain exclusive scan of m words.)
 
 // Copy the sorted survivors into the other pool buffer.

@@ -7,9 +7,11 @@
 // is formed on sm_100a:
 //
 //   * every 16 frames a warp writes its 32 voices x 32 output slots
-//     (16 frames x 2 channels) into its own padded shared-memory tile and
-//     transpose-reduces it: lane l sums row l with four-wide loads, so each
-//     lane ends with one output slot. No block-wide barrier is ever taken.
+//     (16 frames x 2 channels) into its own padded shared-memory tile, one
+//     64-bit (left, right) store per lane and frame, and transpose-reduces
+//     it: lane l sums half a frame row with four-wide loads and trades one
+//     channel with its neighbour, so each lane ends with one output slot.
+//     No block-wide barrier is ever taken.
 //   * each warp owns a 32 KiB slice of the partial buffer (L2-resident); its
 //     later voice batches accumulate into it in batch order.
 //   * a second kernel folds the warps' slices in a fixed order.
@@ -35,8 +37,9 @@ namespace kc {
 struct RenderArgs {
     uint32_t* pool;            // current pool, field-major
     uint32_t cap;              // field stride in words
-    const int16_t* pcm;        // sample pool
-    uint32_t pcm_len;          // i16 frames in it
+    const int16_t* pcm;        // sample pool, i16 as the bank holds it
+    const float* pcmf;         // the same pool converted once to f32 (F32 kernels)
+    uint32_t pcm_len;          // frames in it
     const kc_region_params* params;  // n_slots copies of params_per
     uint32_t params_per;
     uint32_t n_slots;
@@ -54,13 +57,23 @@ struct RenderArgs {
     uint32_t exp_release;
 };
 
-// Sample fetch, CpuSynth::fetch (src/cpu.rs:187-194): i16 / 32767 clamped at
-// -1, out-of-range reads as zero.
-__device__ __forceinline__ float fetch_sample(const int16_t* __restrict__ pcm, uint32_t pcm_len,
-                                              uint32_t base, uint32_t idx) {
+// One in-bounds tap. The f32 pool holds exactly the value CpuSynth::fetch
+// (src/cpu.rs:187-194) computes from the i16 sample -- v / 32767 clamped at
+// -1 -- converted once when the context is created (k_convert_pool), so the
+// conversion leaves the per-frame path; kernels given only the i16 pool
+// (F32 = false) convert per tap.
+template <bool F32>
+__device__ __forceinline__ float tap(const RenderArgs& a, uint32_t i) {
+    if (F32) return __ldg(a.pcmf + i);
+    return fmaxf(__fmul_rn((float)__ldg(a.pcm + i), 1.0f / 32767.0f), -1.0f);
+}
+
+// Sample fetch, CpuSynth::fetch (src/cpu.rs:187-194): out-of-range reads as
+// zero.
+template <bool F32>
+__device__ __forceinline__ float fetch_sample(const RenderArgs& a, uint32_t base, uint32_t idx) {
     const uint32_t i = base + idx;
-    const int16_t v = i < pcm_len ? __ldg(pcm + i) : (int16_t)0;
-    return fmaxf(__fmul_rn((float)v, 1.0f / 32767.0f), -1.0f);
+    return i < a.pcm_len ? tap<F32>(a, i) : 0.0f;
 }
 
 // CpuSynth::advance_index (src/cpu.rs:242-259), general form in i64.
@@ -109,7 +122,7 @@ __device__ __forceinline__ void load_params(VoiceRegs& v, const RenderArgs& a, u
 // Per-frame voice step. Returns the filtered, faded sample y (before the
 // stereo gains). Mirrors src/cpu.rs:490-601 for one frame; the caller has
 // already applied the f < start_rel and DEAD gates.
-template <int INTERP, bool STRICT>
+template <int INTERP, bool STRICT, bool F32>
 __device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, uint32_t f,
                                              bool looping) {
     const uint32_t idx = (uint32_t)(v.phase >> 32);
@@ -147,7 +160,7 @@ __device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, 
     float s;
     const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
     if (INTERP == KC_INTERP_NEAREST) {
-        s = fetch_sample(a.pcm, a.pcm_len, v.base, idx);
+        s = fetch_sample<F32>(a, v.base, idx);
     } else if (INTERP == KC_INTERP_LINEAR) {
         uint32_t i1;
         if (looping) {
@@ -156,8 +169,8 @@ __device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, 
         } else {
             i1 = idx + 1u < v.len ? idx + 1u : v.len - 1u;
         }
-        const float s0 = fetch_sample(a.pcm, a.pcm_len, v.base, idx);
-        const float s1 = fetch_sample(a.pcm, a.pcm_len, v.base, i1);
+        const float s0 = fetch_sample<F32>(a, v.base, idx);
+        const float s1 = fetch_sample<F32>(a, v.base, i1);
         if (STRICT) {
             s = __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac));
         } else {
@@ -167,10 +180,10 @@ __device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, 
         const uint32_t im1 = neighbour(idx, -1, looping, v.ls, v.le, v.len);
         const uint32_t i1 = neighbour(idx, 1, looping, v.ls, v.le, v.len);
         const uint32_t i2 = neighbour(idx, 2, looping, v.ls, v.le, v.len);
-        const float sm1 = fetch_sample(a.pcm, a.pcm_len, v.base, im1);
-        const float s0 = fetch_sample(a.pcm, a.pcm_len, v.base, idx);
-        const float s1 = fetch_sample(a.pcm, a.pcm_len, v.base, i1);
-        const float s2 = fetch_sample(a.pcm, a.pcm_len, v.base, i2);
+        const float sm1 = fetch_sample<F32>(a, v.base, im1);
+        const float s0 = fetch_sample<F32>(a, v.base, idx);
+        const float s1 = fetch_sample<F32>(a, v.base, i1);
+        const float s2 = fetch_sample<F32>(a, v.base, i2);
         // catmull_rom, src/cpu.rs:297-302, left to right, always rounded per op.
         const float ca = __fadd_rn(__fsub_rn(__fadd_rn(__fmul_rn(-0.5f, sm1), __fmul_rn(1.5f, s0)),
                                              __fmul_rn(1.5f, s1)),
@@ -281,14 +294,18 @@ __device__ __forceinline__ bool env_transition(VoiceRegs& v, const RenderArgs& a
 
 // Can this lane run the tile starting at f0 on the fast path? Idle lanes
 // (no voice, dead, or starting after the tile) qualify trivially.
+// NF is the span checked: one 16-frame tile, or the two tiles of a 32-frame
+// gate tile.
+template <uint32_t NF>
 __device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a, uint32_t f0, bool looping,
                                         bool& active) {
+    constexpr uint32_t LOG2 = NF == 32 ? 5 : 4;
     active = false;
-    if (v.stage == ENV_DEAD || v.start_rel >= f0 + MIX_TILE) return true;
-    if (v.start_rel > f0) return false;                       // starts inside the tile
-    if (v.stop_rel != 0u && v.stop_rel <= f0 + MIX_TILE) return false;  // fade begins inside
-    if (v.step >> 59) return false;
-    const uint64_t end = v.phase + (v.step << 4);
+    if (v.stage == ENV_DEAD || v.start_rel >= f0 + NF) return true;
+    if (v.start_rel > f0) return false;                       // starts inside the span
+    if (v.stop_rel != 0u && v.stop_rel <= f0 + NF) return false;  // fade begins inside
+    if (v.step >> (63 - LOG2)) return false;
+    const uint64_t end = v.phase + (v.step << LOG2);
     if (end < v.phase) return false;
     const uint32_t hi = (uint32_t)(end >> 32);
     if (hi == 0xFFFFFFFFu) return false;
@@ -298,113 +315,122 @@ __device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a,
     return true;
 }
 
+// The biquad (transposed direct form II, b2 == b0, src/cpu.rs:564-572) on one
+// sample; y = x when the region's filter is off.
 template <bool STRICT>
+__device__ __forceinline__ float biquad(VoiceRegs& v, float x) {
+    if (!v.filt) return x;
+    float y;
+    if (STRICT) {
+        const float bx = __fmul_rn(v.b0, x);
+        y = __fadd_rn(bx, v.z1);
+        v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
+        v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
+    } else {
+        y = fmaf(v.b0, x, v.z1);
+        v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
+        v.z2 = fmaf(v.b0, x, -(v.a2 * y));
+    }
+    return y;
+}
+
+template <bool STRICT>
+__device__ __forceinline__ float lerp(float s0, float s1, float frac) {
+    return STRICT ? __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac)) : fmaf(s1 - s0, frac, s0);
+}
+
+template <bool STRICT, bool F32>
 __device__ __forceinline__ float fast_frame(VoiceRegs& v, const RenderArgs& a, EnvStep& e, bool& active) {
     // Envelope, exactly rounded in one FMA.
     v.level = __fmaf_rn(v.level, e.em, e.ea);
     if (__fmul_rn(e.sgn, v.level) >= e.thr) active = env_transition(v, a, e);
     // Linear interpolation between two adjacent, in-bounds taps.
-    const uint32_t idx = (uint32_t)(v.phase >> 32);
-    const int16_t* p = a.pcm + (v.base + idx);
-    const float s0 = fmaxf(__fmul_rn((float)__ldg(p), 1.0f / 32767.0f), -1.0f);
-    const float s1 = fmaxf(__fmul_rn((float)__ldg(p + 1), 1.0f / 32767.0f), -1.0f);
+    const uint32_t i0 = v.base + (uint32_t)(v.phase >> 32);
+    const float s0 = tap<F32>(a, i0);
+    const float s1 = tap<F32>(a, i0 + 1u);
     const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
-    const float s = STRICT ? __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac)) : fmaf(s1 - s0, frac, s0);
-    const float x = __fmul_rn(s, fminf(v.level, 1.0f));
-    float y = x;
-    if (v.filt) {
-        if (STRICT) {
-            const float bx = __fmul_rn(v.b0, x);
-            y = __fadd_rn(bx, v.z1);
-            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
-            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
-        } else {
-            y = fmaf(v.b0, x, v.z1);
-            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
-            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
-        }
-    }
+    const float y = biquad<STRICT>(v, __fmul_rn(lerp<STRICT>(s0, s1, frac), fminf(v.level, 1.0f)));
     v.phase += v.step;
     return y;
 }
 
 // The hot path: a tile in which no lane is idle and no envelope transition
 // can happen. `no_transition` is conservative: it proves, with a margin far
-// above the rounding of 16 sequential steps (16 roundings of at most half an
-// ulp each, about 1e-6 relative), that the threshold cannot be crossed inside
-// the tile. When it holds, the frame is branch-free and the compiler can
-// overlap consecutive frames (and the lane's voices).
+// above the rounding of NF sequential steps (at most 32 roundings of half an
+// ulp each, about 2e-6 relative), that the threshold cannot be crossed inside
+// the span. It only accepts monotone steps (a non-negative attack rate; a
+// decay or release that multiplies by a coefficient in [0, 1] or subtracts a
+// non-negative one, from a non-negative level), so the last frame's level
+// bounds every frame's. When it holds, the frame is branch-free and the
+// compiler can overlap consecutive frames (and the lane's voices).
+template <uint32_t NF>
 __device__ __forceinline__ bool no_transition(const VoiceRegs& v, const EnvStep& e) {
+    constexpr float N = (float)NF;
     if (v.stage == ENV_SUSTAIN) return true;
     if (v.stage == ENV_ATTACK) {
         // level grows by attack_rate per frame towards attack_end
-        return v.level + 16.0f * e.ea + 1.0e-5f * fabsf(e.thr) < e.thr;
+        return e.ea >= 0.0f && v.level + N * e.ea + 1.0e-5f * fabsf(e.thr) < e.thr;
     }
     const float thr = -e.thr;  // decay target or floor
+    if (!(v.level >= 0.0f)) return false;
     if (e.em != 1.0f) {
-        float m = e.em * e.em;  // em^16 by squaring
+        if (!(e.em >= 0.0f && e.em <= 1.0f)) return false;
+        float m = e.em * e.em;  // em^NF by squaring
         m *= m;
         m *= m;
         m *= m;
+        if (NF == 32) m *= m;
         return v.level * m * (1.0f - 1.0e-5f) > thr;
     }
-    return v.level + 16.0f * e.ea - 1.0e-5f * v.level > thr;  // linear: ea = -coef
+    return e.ea <= 0.0f && v.level + N * e.ea - 1.0e-5f * v.level > thr;  // linear: ea = -coef
 }
 
-template <bool STRICT>
+// Under no_transition, is min(level, 1) == level on every frame of the tile?
+// An attack stays below attack_end; every other accepted step is
+// non-increasing from the tile's first level.
+__device__ __forceinline__ bool level_at_most_one(const VoiceRegs& v, const EnvStep& e) {
+    if (v.stage == ENV_ATTACK) return e.thr <= 1.0f;
+    return v.level <= 1.0f;
+}
+
+// A hot frame with a fractional phase: two taps and the lerp.
+template <bool STRICT, bool F32>
 __device__ __forceinline__ float hot_frame(VoiceRegs& v, const RenderArgs& a, const EnvStep& e) {
     v.level = __fmaf_rn(v.level, e.em, e.ea);
-    const uint32_t idx = (uint32_t)(v.phase >> 32);
-    const int16_t* p = a.pcm + (v.base + idx);
-    const float s0 = fmaxf(__fmul_rn((float)__ldg(p), 1.0f / 32767.0f), -1.0f);
-    const float s1 = fmaxf(__fmul_rn((float)__ldg(p + 1), 1.0f / 32767.0f), -1.0f);
+    const uint32_t i0 = v.base + (uint32_t)(v.phase >> 32);
+    const float s0 = tap<F32>(a, i0);
+    const float s1 = tap<F32>(a, i0 + 1u);
     const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
-    const float s = STRICT ? __fadd_rn(s0, __fmul_rn(__fsub_rn(s1, s0), frac)) : fmaf(s1 - s0, frac, s0);
-    const float x = __fmul_rn(s, fminf(v.level, 1.0f));
-    float y = x;
-    if (v.filt) {
-        if (STRICT) {
-            const float bx = __fmul_rn(v.b0, x);
-            y = __fadd_rn(bx, v.z1);
-            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
-            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
-        } else {
-            y = fmaf(v.b0, x, v.z1);
-            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
-            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
-        }
-    }
+    const float y = biquad<STRICT>(v, __fmul_rn(lerp<STRICT>(s0, s1, frac), v.level));
     v.phase += v.step;
     return y;
 }
 
-// The hot path when every lane's phase and step have a zero fraction (an
+// A hot frame when every lane's phase and step have a zero fraction (an
 // exactly integer pitch ratio: the root key played at the pool rate, or whole
 // octaves of it). Then frac is 0 for every frame of the tile, and the linear
 // interpolation s0 + (s1 - s0) * 0 is exactly s0 (s0 is never -0: it is
 // v / 32767 clamped at -1, so +0 for a zero tap), in both the strict and the
-// fused form. The second tap, its conversion and the lerp drop out.
-template <bool STRICT>
-__device__ __forceinline__ float hot_frame_int(VoiceRegs& v, const RenderArgs& a, const EnvStep& e) {
+// fused form; nearest interpolation reads the same tap. The second tap, its
+// conversion and the lerp drop out, and the phase advances by the step's
+// integer part alone (`off` = base + phase_hi; the tile's phase is written
+// back once at its end).
+template <bool STRICT, bool F32>
+__device__ __forceinline__ float hot_frame_int(VoiceRegs& v, const RenderArgs& a, const EnvStep& e, uint32_t& off) {
     v.level = __fmaf_rn(v.level, e.em, e.ea);
-    const uint32_t idx = (uint32_t)(v.phase >> 32);
-    const float s = fmaxf(__fmul_rn((float)__ldg(a.pcm + (v.base + idx)), 1.0f / 32767.0f), -1.0f);
-    const float x = __fmul_rn(s, fminf(v.level, 1.0f));
-    float y = x;
-    if (v.filt) {
-        if (STRICT) {
-            const float bx = __fmul_rn(v.b0, x);
-            y = __fadd_rn(bx, v.z1);
-            v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
-            v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
-        } else {
-            y = fmaf(v.b0, x, v.z1);
-            v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
-            v.z2 = fmaf(v.b0, x, -(v.a2 * y));
-        }
-    }
-    v.phase += v.step;  // the fraction stays zero
+    const float y = biquad<STRICT>(v, __fmul_rn(tap<F32>(a, off), v.level));
+    off += (uint32_t)(v.step >> 32);
     return y;
+}
+
+// A hot frame of a voice whose step is exactly 1.0 (the sample played at its
+// root pitch at the pool rate -- every unbent note of a bank sampled per key):
+// frame i of the tile reads tap i past the tile's first, a fixed offset.
+template <bool STRICT, bool F32>
+__device__ __forceinline__ float hot_frame_unit(VoiceRegs& v, const RenderArgs& a, const EnvStep& e, uint32_t off0,
+                                                uint32_t i) {
+    v.level = __fmaf_rn(v.level, e.em, e.ea);
+    return biquad<STRICT>(v, __fmul_rn(tap<F32>(a, off0 + i), v.level));
 }
 
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
@@ -414,8 +440,16 @@ __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 }
 
 constexpr uint32_t RENDER_WARPS = 8;        // warps per CTA
-constexpr uint32_t SM_ROW = 36;             // padded row of the warp tile (floats)
-constexpr uint32_t SM_WARP = 32 * SM_ROW;   // floats per warp tile
+// The warp's mix tile: one row per frame of the 16-frame tile, each row the
+// 32 lanes' (left, right) pairs -- lanes 0-15 at floats 0-31, lanes 16-31 at
+// floats 36-67 -- in a 72-float row. A lane stores its pair with one 64-bit
+// store (each half-warp writes 128 contiguous bytes); for the fold, lane l
+// reads half (l & 1) of row (l >> 1) with four-wide loads, and the 8 lanes of
+// each quarter-warp phase land on 8 distinct 4-bank groups
+// ((72 * row + 36 * half) mod 32 = 8 * row + 4 * half).
+constexpr uint32_t SM_ROW = 72;             // floats per frame row
+constexpr uint32_t SM_HALF = 36;            // offset of lanes 16-31 in a row
+constexpr uint32_t SM_WARP = MIX_TILE * SM_ROW;   // floats per warp tile
 
 // Load one voice's state into registers (the reference loads the same fields,
 // shaders/render.wgsl:203-237).
@@ -520,11 +554,50 @@ __device__ __forceinline__ void acc_out(float& yl, float& yr, float y, const Voi
     }
 }
 
+// The paths a tile can take, fastest first.
+constexpr int P_UNIT = 0, P_INT = 1, P_HOT = 2, P_FAST = 3, P_GENERAL = 4;
+
+// Classify the NF frames from f0 for the whole warp: ok (linear: every lane
+// on the fast path), hot (no idle lane, no transition, level <= 1
+// throughout), integral (zero phase fractions), unit (step exactly 1.0).
+// Fills the per-voice looping/active flags and envelope constants the paths
+// use. Warp-uniform result.
+template <int INTERP, int V, uint32_t NF>
+__device__ __forceinline__ int classify(const VoiceRegs (&v)[V], const RenderArgs& a, uint32_t f0, bool (&looping)[V],
+                                        bool (&active)[V], EnvStep (&e)[V]) {
+    constexpr bool FASTPATHS = INTERP != KC_INTERP_CUBIC;
+    bool ok = FASTPATHS;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        looping[k] = v[k].loop_en && !(v[k].lur && v[k].stage >= ENV_RELEASE);
+        active[k] = false;
+        if (FASTPATHS) ok = fast_ok<NF>(v[k], a, f0, looping[k], active[k]) && ok;
+    }
+    bool hot = ok, integral = true, unit = true;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        e[k] = env_constants(v[k], a);
+        hot = hot && active[k] && no_transition<NF>(v[k], e[k]) && level_at_most_one(v[k], e[k]);
+        integral = integral && ((uint32_t)v[k].phase | (uint32_t)v[k].step) == 0u;
+        unit = unit && v[k].step == (1ull << 32);
+    }
+    if (FASTPATHS && __all_sync(0xFFFFFFFFu, hot && integral && unit)) return P_UNIT;
+    if (FASTPATHS && __all_sync(0xFFFFFFFFu, hot && integral)) return P_INT;
+    if (INTERP == KC_INTERP_LINEAR && __all_sync(0xFFFFFFFFu, hot)) return P_HOT;
+    if (INTERP == KC_INTERP_LINEAR && __all_sync(0xFFFFFFFFu, ok)) return P_FAST;
+    return P_GENERAL;
+}
+
+// This lane's (left, right) pair for frame i of the tile.
+__device__ __forceinline__ void put_pair(float* sm, uint32_t lane, uint32_t i, float yl, float yr) {
+    *reinterpret_cast<float2*>(sm + i * SM_ROW + (lane >> 4) * SM_HALF + (lane & 15u) * 2u) = make_float2(yl, yr);
+}
+
 // Render every batch of 32*V voices this warp owns. Lane l of batch b holds
 // voices b*32V + k*32 + l for k < V, so each of the V loads per field is one
 // coalesced line, and its V voices' frames are summed in k order before the
-// warp transpose-reduce.
-template <int INTERP, bool CHAN, bool STRICT, int MIX, int V>
+// warp transpose-reduce. F32 selects the pre-converted f32 sample pool.
+template <int INTERP, bool CHAN, bool STRICT, int MIX, int V, bool F32 = true>
 __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, uint32_t gw, uint32_t tw, uint32_t n) {
     const uint32_t lane = lane_id();
     const uint32_t per = 32u * V;
@@ -536,6 +609,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
     // KC_MIX_F64: the same buffer holds one slice of doubles per warp.
     double* __restrict__ part_d = MIX == KC_MIX_F64 ? reinterpret_cast<double*>(a.partial) + (size_t)gw * samples
                                                     : nullptr;
+    constexpr bool FASTPATHS = INTERP != KC_INTERP_CUBIC;
 
     for (uint32_t b = gw; b < nbatch; b += tw) {
         VoiceRegs v[V];
@@ -546,45 +620,73 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
         }
         const bool first = b == gw;
 
+        // A tile's path comes from classifying it alone, or -- at the start
+        // of a 32-frame gate tile -- both of its tiles at once: when the
+        // whole span is hot, the second tile reuses the result (and the
+        // envelope constants, which no hot frame changes).
+        EnvStep e[V];
+        bool looping[V], active[V];
+        int carried = -1;
+        uint32_t next_gate = 0, gt = 0;
+        const bool span32 = a.gate_frames % 32u == 0u;
         for (uint32_t f0 = 0; f0 < a.block_frames; f0 += MIX_TILE) {
-            if (f0 % a.gate_frames == 0u) {
-                const uint32_t gt = f0 / a.gate_frames;
+            if (f0 == next_gate) {
 #pragma unroll
                 for (int k = 0; k < V; ++k) tile_update<CHAN>(v[k], a, gt, chan_active);
+                ++gt;
+                next_gate += a.gate_frames;
             }
-            bool looping[V], active[V];
-            bool ok = INTERP == KC_INTERP_LINEAR;
-#pragma unroll
-            for (int k = 0; k < V; ++k) {
-                looping[k] = v[k].loop_en && !(v[k].lur && v[k].stage >= ENV_RELEASE);
-                active[k] = false;
-                if (INTERP == KC_INTERP_LINEAR) ok = fast_ok(v[k], a, f0, looping[k], active[k]) && ok;
+            int path;
+            if (carried >= 0) {
+                path = carried;
+                carried = -1;
+            } else {
+                path = P_GENERAL;
+                if (span32 && (f0 & 31u) == 0u) {
+                    path = classify<INTERP, V, 32>(v, a, f0, looping, active, e);
+                    if (path <= P_HOT) carried = path;
+                }
+                if (carried < 0) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e);
             }
-            EnvStep e[V];
-            bool hot = ok;
+            if (FASTPATHS && path == P_UNIT) {
+                // Unit steps, zero fractions: tap i of the tile is a fixed
+                // offset from the tile's first.
+                uint32_t off[V];
 #pragma unroll
-            for (int k = 0; k < V; ++k) {
-                e[k] = env_constants(v[k], a);
-                hot = hot && active[k] && no_transition(v[k], e[k]);
-            }
-            bool integral = true;
-#pragma unroll
-            for (int k = 0; k < V; ++k) integral = integral && ((uint32_t)v[k].phase | (uint32_t)v[k].step) == 0u;
-            if (INTERP == KC_INTERP_LINEAR && __all_sync(0xFFFFFFFFu, hot && integral)) {
-                // Straight-line frames with a zero phase fraction.
+                for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
 #pragma unroll
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
                     float yl, yr;
 #pragma unroll
                     for (int k = 0; k < V; ++k) {
-                        const float y = hot_frame_int<STRICT>(v[k], a, e[k]);
+                        const float y = hot_frame_unit<STRICT, F32>(v[k], a, e[k], off[k], i);
                         if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
                         else acc_out<STRICT, false>(yl, yr, y, v[k]);
                     }
-                    sm[(2u * i) * SM_ROW + lane] = yl;
-                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                    put_pair(sm, lane, i, yl, yr);
                 }
-            } else if (__all_sync(0xFFFFFFFFu, hot)) {
+#pragma unroll
+                for (int k = 0; k < V; ++k) v[k].phase += (uint64_t)MIX_TILE << 32;
+            } else if (FASTPATHS && path == P_INT) {
+                // Straight-line frames with a zero phase fraction.
+                uint32_t off[V];
+#pragma unroll
+                for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
+#pragma unroll
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    float yl, yr;
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        const float y = hot_frame_int<STRICT, F32>(v[k], a, e[k], off[k]);
+                        if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                        else acc_out<STRICT, false>(yl, yr, y, v[k]);
+                    }
+                    put_pair(sm, lane, i, yl, yr);
+                }
+                // fast_ok proved phase + 16 * step does not overflow
+#pragma unroll
+                for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
+            } else if (INTERP == KC_INTERP_LINEAR && path == P_HOT) {
                 // Every lane's every voice is live for the whole tile with no
                 // stage change: straight-line code, no branches.
 #pragma unroll
@@ -592,27 +694,25 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                     float yl, yr;
 #pragma unroll
                     for (int k = 0; k < V; ++k) {
-                        const float y = hot_frame<STRICT>(v[k], a, e[k]);
+                        const float y = hot_frame<STRICT, F32>(v[k], a, e[k]);
                         if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
                         else acc_out<STRICT, false>(yl, yr, y, v[k]);
                     }
-                    sm[(2u * i) * SM_ROW + lane] = yl;
-                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                    put_pair(sm, lane, i, yl, yr);
                 }
-            } else if (__all_sync(0xFFFFFFFFu, ok)) {
+            } else if (INTERP == KC_INTERP_LINEAR && path == P_FAST) {
 #pragma unroll
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
                     float yl = 0.0f, yr = 0.0f;
 #pragma unroll
                     for (int k = 0; k < V; ++k) {
                         if (active[k]) {
-                            const float y = fast_frame<STRICT>(v[k], a, e[k], active[k]);
+                            const float y = fast_frame<STRICT, F32>(v[k], a, e[k], active[k]);
                             if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
                             else acc_out<STRICT, false>(yl, yr, y, v[k]);
                         }
                     }
-                    sm[(2u * i) * SM_ROW + lane] = yl;
-                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                    put_pair(sm, lane, i, yl, yr);
                 }
             } else {
 #pragma unroll 1
@@ -622,55 +722,77 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
 #pragma unroll
                     for (int k = 0; k < V; ++k) {
                         if (v[k].stage != ENV_DEAD && f >= v[k].start_rel) {
-                            const float y = voice_frame<INTERP, STRICT>(v[k], a, f, looping[k]);
+                            const float y = voice_frame<INTERP, STRICT, F32>(v[k], a, f, looping[k]);
                             if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
                             else acc_out<STRICT, false>(yl, yr, y, v[k]);
                         }
                     }
-                    sm[(2u * i) * SM_ROW + lane] = yl;
-                    sm[(2u * i + 1u) * SM_ROW + lane] = yr;
+                    put_pair(sm, lane, i, yl, yr);
                 }
             }
             __syncwarp();
-            // Lane l folds row l (one output slot over the warp's voices).
-            const float4* row = reinterpret_cast<const float4*>(sm + lane * SM_ROW);
-            float4 q[8];
-#pragma unroll
-            for (int c = 0; c < 8; ++c) q[c] = row[c];
-            __syncwarp();
+            // Lane l owns output slot l of the tile: frame l >> 1, channel
+            // l & 1, summed over the warp's 32 lanes.
             const uint32_t j = f0 * 2u + lane;
+            const uint32_t h = lane & 1u;
+            const float* row = sm + (lane >> 1) * SM_ROW;
             if (MIX == KC_MIX_F32_TREE) {
-                float r[8];
+                // Half h of the row: lanes 16h..16h+15, two lanes per float4.
+                // Sum both channels over the half in a fixed tree, then swap
+                // the channel this lane does not own with its neighbour: each
+                // slot is (lanes 0-15) + (lanes 16-31), in that order.
+                // (Two passes of four loads keep fewer registers live.)
+                const float4* q4 = reinterpret_cast<const float4*>(row + h * SM_HALF);
+                float rl[4], rr[4];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) r[c] = __fadd_rn(__fadd_rn(q[c].x, q[c].y), __fadd_rn(q[c].z, q[c].w));
-                const float sum = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
-                                            __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
-                part[j] = first ? sum : __fadd_rn(part[j], sum);
-            } else if (MIX == KC_MIX_F64) {
-                // The FP64 form: the row's 32 f32 terms summed in double.
-                double r[8];
+                for (int p = 0; p < 2; ++p) {
+                    float4 q[4];
 #pragma unroll
-                for (int c = 0; c < 8; ++c)
-                    r[c] = ((double)q[c].x + (double)q[c].y) + ((double)q[c].z + (double)q[c].w);
-                const double sum = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-                part_d[j] = first ? sum : part_d[j] + sum;
-            } else {
-                // Compensated: sequential two-sum over the row with carries.
-                float s = q[0].x, e = 0.0f, t, err;
-                const float* qq = reinterpret_cast<const float*>(q);
+                    for (int c = 0; c < 4; ++c) q[c] = q4[4 * p + c];
 #pragma unroll
-                for (int c = 1; c < 32; ++c) {
-                    two_sum(s, qq[c], t, err);
-                    s = t;
-                    e = __fadd_rn(e, err);
+                    for (int c = 0; c < 2; ++c) {
+                        rl[2 * p + c] = __fadd_rn(__fadd_rn(q[2 * c].x, q[2 * c].z), __fadd_rn(q[2 * c + 1].x, q[2 * c + 1].z));
+                        rr[2 * p + c] = __fadd_rn(__fadd_rn(q[2 * c].y, q[2 * c].w), __fadd_rn(q[2 * c + 1].y, q[2 * c + 1].w));
+                    }
                 }
-                if (first) {
-                    part[j] = s;
-                    part_c[j] = e;
+                __syncwarp();
+                const float sl = __fadd_rn(__fadd_rn(rl[0], rl[1]), __fadd_rn(rl[2], rl[3]));
+                const float sr = __fadd_rn(__fadd_rn(rr[0], rr[1]), __fadd_rn(rr[2], rr[3]));
+                const float mine = h ? sr : sl;
+                const float theirs = __shfl_xor_sync(0xFFFFFFFFu, h ? sl : sr, 1);
+                const float sum = __fadd_rn(theirs, mine);  // (half 0) + (half 1) either way
+                part[j] = first ? sum : __fadd_rn(part[j], sum);
+            } else {
+                // This lane's channel over all 32 lanes, in lane order.
+                float qq[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c) qq[c] = row[(c >> 4) * SM_HALF + (c & 15) * 2 + h];
+                __syncwarp();
+                if (MIX == KC_MIX_F64) {
+                    // The FP64 form: the slot's 32 f32 terms summed in double.
+                    double r[8];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        r[c] = ((double)qq[4 * c] + (double)qq[4 * c + 1]) + ((double)qq[4 * c + 2] + (double)qq[4 * c + 3]);
+                    const double sum = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+                    part_d[j] = first ? sum : part_d[j] + sum;
                 } else {
-                    two_sum(part[j], s, t, err);
-                    part[j] = t;
-                    part_c[j] = __fadd_rn(__fadd_rn(part_c[j], e), err);
+                    // Compensated: sequential two-sum over the slot with carries.
+                    float s = qq[0], e = 0.0f, t, err;
+#pragma unroll
+                    for (int c = 1; c < 32; ++c) {
+                        two_sum(s, qq[c], t, err);
+                        s = t;
+                        e = __fadd_rn(e, err);
+                    }
+                    if (first) {
+                        part[j] = s;
+                        part_c[j] = e;
+                    } else {
+                        two_sum(part[j], s, t, err);
+                        part[j] = t;
+                        part_c[j] = __fadd_rn(__fadd_rn(part_c[j], e), err);
+                    }
                 }
             }
         }

@@ -12,6 +12,8 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -35,6 +37,16 @@ int fail(int code, const std::string& msg) {
 using Clock = std::chrono::steady_clock;
 
 double since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+// KESTREL_SERVE_TRACE=1: one stderr line per batch step (or per sequential
+// job) with the phase times, for following a long run.
+bool trace_on() {
+    static const bool on = [] {
+        const char* v = std::getenv("KESTREL_SERVE_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
 
 // A fixed set of threads running queued tasks; parallel_for lets the caller
 // take part and returns when every index is done.
@@ -77,10 +89,15 @@ public:
         const size_t helpers = std::min<size_t>(th_.size(), n - 1);
         for (size_t k = 0; k < helpers; ++k) run(body);
         body();
-        std::unique_lock<std::mutex> g(dm);
-        dcv.wait(g, [&] { return left.load() == 0; });
-        // Helpers that found no index may still be inside body(); they only
-        // touch `next`, so wait for them before the locals go away.
+        {
+            // Released before the idle wait below: the helper that finished
+            // the last index takes this lock to notify, and it must be able
+            // to, or it never goes idle.
+            std::unique_lock<std::mutex> g(dm);
+            dcv.wait(g, [&] { return left.load() == 0; });
+        }
+        // Helpers may still be inside body() (notifying, or having found no
+        // index); wait for them before the locals they use go away.
         std::unique_lock<std::mutex> g2(m_);
         idle_cv_.wait(g2, [&] { return q_.empty() && busy_ == 0; });
     }
@@ -183,7 +200,9 @@ int create(Job& j) {
         j.err = kc_last_error();
         return rc;
     }
-    j.res->device_bytes = kc_synth_device_bytes(j.synth);
+    // Charge the most the context can grow to (its spawn buffer follows the
+    // largest block), never less than what it holds now.
+    j.res->device_bytes = std::max<uint64_t>(j.est_bytes, kc_synth_device_bytes(j.synth));
     return KC_OK;
 }
 
@@ -228,8 +247,9 @@ int finish(Job& j, const ks_server_config& sc, double now) {
 
 bool same_batch_variant(const kc_config& a, const kc_config& b) {
     const uint32_t va = a.voices_per_lane == 2 ? 2 : 1, vb = b.voices_per_lane == 2 ? 2 : 1;
+    const uint32_t ra = a.sort_radix_bits ? a.sort_radix_bits : 8, rb = b.sort_radix_bits ? b.sort_radix_bits : 8;
     return a.device == b.device && a.block_frames == b.block_frames && a.interpolation == b.interpolation &&
-           (a.strict_fp != 0) == (b.strict_fp != 0) && a.mix_mode == b.mix_mode && va == vb;
+           (a.strict_fp != 0) == (b.strict_fp != 0) && a.mix_mode == b.mix_mode && va == vb && ra == rb;
 }
 
 int serve_sequential(const ks_server_config& sc, std::vector<Job>& jobs, const std::vector<uint32_t>& order,
@@ -265,6 +285,9 @@ int serve_sequential(const ks_server_config& sc, std::vector<Job>& jobs, const s
         }
         j.res->done_s = since(t0);
         j.res->status = j.status;
+        if (trace_on())
+            std::fprintf(stderr, "[serve] t=%.3f job=%u blocks=%llu setup_s=%.3f run_s=%.3f status=%d\n", since(t0), j.id,
+                         (unsigned long long)j.res->blocks, j.res->setup_s, j.res->done_s - j.res->admit_s, j.status);
         release(j);
     }
     return KC_OK;
@@ -293,6 +316,7 @@ int serve_batched(const ks_server_config& sc, std::vector<Job>& jobs, const std:
     bc.strict_fp = c0.strict_fp;
     bc.mix_mode = c0.mix_mode;
     bc.voices_per_lane = c0.voices_per_lane == 2 ? 2 : 1;
+    bc.sort_radix_bits = c0.sort_radix_bits;
     bc.use_graph = sc.use_graph;
     kc_batch* batch = nullptr;
     if (int rc = kc_batch_create(&bc, &batch)) return fail(rc, kc_last_error());
@@ -378,6 +402,7 @@ int serve_batched(const ks_server_config& sc, std::vector<Job>& jobs, const std:
             }
         }
         rs.max_resident = std::max<uint32_t>(rs.max_resident, (uint32_t)resident.size());
+        const auto t_step = Clock::now();
         // Prepare every resident job's block.
         prc.assign(resident.size(), KC_OK);
         step_pool->parallel_for(resident.size(), [&](size_t k) {
@@ -422,6 +447,10 @@ int serve_batched(const ks_server_config& sc, std::vector<Job>& jobs, const std:
                         j.finished = true;
                     }
                 });
+                if (trace_on())
+                    std::fprintf(stderr, "[serve] t=%.3f step=%llu resident=%zu gpu_ms=%.2f step_ms=%.2f used_gb=%.2f "
+                                 "done=%zu/%zu\n", since(t0), (unsigned long long)rs.steps, stepping.size(), ms,
+                                 since(t_step) * 1e3, used / 1e9, completed, jobs.size());
             }
         }
         // Retire finished jobs; their memory is free for the next admission.
@@ -442,9 +471,184 @@ int serve_batched(const ks_server_config& sc, std::vector<Job>& jobs, const std:
     return rc_out;
 }
 
+// ---- autotuner ----------------------------------------------------------------
+
+// One block's inputs copied out of the driver.
+struct Recorded {
+    std::vector<uint32_t> gates, chan;
+    std::vector<kc_spawn_cmd> cmds;
+    std::vector<std::pair<uint32_t, std::vector<kc_region_params>>> variants;
+    int bend = 0, gain = 0, variant = 0;
+};
+
+int record_block(kh_driver* drv, uint32_t live, Recorded& r) {
+    kh_block b{};
+    if (kh_driver_prepare(drv, live, &b)) return fail(KC_ERR_INVALID, std::string("prepare: ") + kh_last_error());
+    r.gates.assign(b.gates, b.gates + b.n_gates);
+    r.chan.assign(b.chan, b.chan + b.n_chan);
+    r.cmds.assign(b.cmds, b.cmds + b.n_cmds);
+    r.bend = b.bend;
+    r.gain = b.gain;
+    r.variant = b.variant;
+    r.variants.clear();
+    for (uint32_t i = 0; i < b.n_variants; ++i) {
+        uint32_t idx = 0;
+        const kc_region_params* data = nullptr;
+        size_t n = 0;
+        if (kh_driver_variant(drv, i, &idx, &data, &n)) return fail(KC_ERR_INVALID, kh_last_error());
+        r.variants.emplace_back(idx, std::vector<kc_region_params>(data, data + n));
+    }
+    return KC_OK;
+}
+
+int feed_block(kc_synth* s, const Recorded& r) {
+    for (const auto& v : r.variants)
+        if (int rc = kc_set_params_variant(s, v.first, v.second.data(), v.second.size())) return fail(rc, kc_last_error());
+    if (int rc = kc_set_gates(s, r.gates.data(), r.gates.size())) return fail(rc, kc_last_error());
+    if (int rc = kc_set_channels(s, r.chan.data(), r.chan.size(), r.bend, r.gain, r.variant))
+        return fail(rc, kc_last_error());
+    if (int rc = kc_spawn(s, r.cmds.data(), r.cmds.size())) return fail(rc, kc_last_error());
+    return KC_OK;
+}
+
+// Render one recorded block; returns the voices it rendered.
+int render_recorded(kc_synth* s, const Recorded& r, std::vector<float>& out, uint32_t* rendered) {
+    if (int rc = feed_block(s, r)) return rc;
+    if (int rc = kc_render(s, out.data(), out.size())) return fail(rc, kc_last_error());
+    if (int rc = kc_last_block_voices(s, rendered)) return fail(rc, kc_last_error());
+    return KC_OK;
+}
+
+struct Owned {
+    kh_bank* bank = nullptr;
+    kh_driver* drv = nullptr;
+    kc_synth* snap = nullptr;
+    kc_synth* live = nullptr;
+    ~Owned() {
+        if (live) kc_synth_destroy(live);
+        if (snap) kc_synth_destroy(snap);
+        if (drv) kh_driver_destroy(drv);
+        if (bank) kh_bank_destroy(bank);
+    }
+};
+
+// Tune one block length: pre-roll, snapshot, record, replay per candidate.
+int tune_block_length(const ks_job_spec& job, uint32_t bf, const std::vector<uint32_t>& vpls,
+                      const std::vector<uint32_t>& radices, uint32_t preroll, uint32_t timed,
+                      std::vector<ks_tune_result>& out) {
+    kc_config cfg = job.cfg;
+    cfg.block_frames = bf;
+    cfg.voices_per_lane = 0;
+    cfg.sort_radix_bits = 0;
+    Owned o;
+    o.bank = kh_bank_synthetic(&job.bank, &cfg, &job.opt);
+    if (!o.bank) return fail(KC_ERR_INVALID, std::string("bank: ") + kh_last_error());
+    o.drv = kh_driver_open(&cfg, &job.opt, o.bank, &job.midi);
+    if (!o.drv) return fail(KC_ERR_INVALID, std::string("driver: ") + kh_last_error());
+    const int16_t* pool = nullptr;
+    uint64_t pool_len = 0;
+    const kc_region_params* params = nullptr;
+    uint32_t n_params = 0;
+    kh_bank_pool(o.bank, &pool, &pool_len);
+    kh_bank_params(o.bank, &params, &n_params);
+    if (int rc = kc_synth_create(&cfg, pool, pool_len, params, n_params, kh_bank_regions(o.bank),
+                                 kh_bank_max_sample_len(o.bank), &o.live))
+        return fail(rc, kc_last_error());
+    std::vector<float> buf((size_t)bf * 2);
+    Recorded r;
+    uint32_t live = 0, rendered = 0;
+    int more = 1;
+    kc_block_stats st{};
+    for (uint32_t i = 0; i < preroll && more; ++i) {
+        if (int rc = record_block(o.drv, live, r)) return rc;
+        if (int rc = render_recorded(o.live, r, buf, &rendered)) return rc;
+        kc_stats(o.live, &st);
+        live = (uint32_t)std::min<uint64_t>(st.active_voices, 0xFFFFFFFFu);
+        if (kh_driver_finish(o.drv, st.active_voices, &more)) return fail(KC_ERR_INVALID, kh_last_error());
+    }
+    if (int rc = kc_synth_clone(o.live, &o.snap)) return fail(rc, kc_last_error());
+    std::vector<Recorded> rec;
+    // One more block than timed: each candidate renders the first untimed,
+    // so its kernels are loaded before the clock starts.
+    for (uint32_t i = 0; i < timed + 1 && more; ++i) {
+        rec.emplace_back();
+        if (int rc = record_block(o.drv, live, rec.back())) return rc;
+        if (int rc = render_recorded(o.live, rec.back(), buf, &rendered)) return rc;
+        kc_stats(o.live, &st);
+        live = (uint32_t)std::min<uint64_t>(st.active_voices, 0xFFFFFFFFu);
+        if (kh_driver_finish(o.drv, st.active_voices, &more)) return fail(KC_ERR_INVALID, kh_last_error());
+    }
+    if (rec.empty()) return fail(KC_ERR_INVALID, "the job ended before any block could be timed");
+    for (uint32_t v : vpls) {
+        for (uint32_t rb : radices) {
+            kc_config c = cfg;
+            c.voices_per_lane = v;
+            c.sort_radix_bits = rb;
+            kc_synth* k = nullptr;
+            if (int rc = kc_synth_clone_config(o.snap, &c, &k)) return fail(rc, kc_last_error());
+            ks_tune_result res{};
+            res.voices_per_lane = v;
+            res.sort_radix_bits = rb;
+            res.block_frames = bf;
+            int rc = KC_OK;
+            const size_t first_timed = rec.size() > 1 ? 1 : 0;
+            for (size_t i = 0; i < rec.size() && rc == KC_OK; ++i) {
+                if (i == first_timed) rc = kc_set_profile(k, 1);
+                if (rc == KC_OK) rc = render_recorded(k, rec[i], buf, &rendered);
+                if (i >= first_timed) res.voice_samples += (uint64_t)rendered * bf;
+            }
+            double ms[8] = {};
+            uint64_t blocks = 0;
+            if (rc == KC_OK && (rc = kc_timings_total(k, ms, 8, &blocks)) != KC_OK) fail(rc, kc_last_error());
+            kc_synth_destroy(k);
+            if (rc) return rc;
+            for (double m : ms) res.device_ms += m;
+            res.blocks = (uint32_t)blocks;
+            res.voice_samples_per_s = res.device_ms > 0 ? res.voice_samples / (res.device_ms * 1e-3) : 0.0;
+            out.push_back(res);
+        }
+    }
+    return KC_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int ks_autotune(const ks_job_spec* job, const ks_tune_space* space, kc_config* best, ks_tune_result* results,
+                uint32_t cap, uint32_t* n) {
+    if (!job || !best) return fail(KC_ERR_INVALID, "null argument");
+    ks_tune_space sp{};
+    if (space) sp = *space;
+    std::vector<uint32_t> vpls, radices, lengths;
+    const uint32_t vmask = sp.voices_per_lane_mask ? sp.voices_per_lane_mask : 3u;
+    for (uint32_t v = 1; v <= 2; ++v)
+        if (vmask & (1u << (v - 1))) vpls.push_back(v);
+    const uint32_t rmask = sp.radix_mask ? sp.radix_mask : ((1u << 6) | (1u << 8) | (1u << 10));
+    for (uint32_t r = 4; r <= 10; ++r)
+        if (rmask & (1u << r)) radices.push_back(r);
+    for (uint32_t bf : sp.block_frames)
+        if (bf) lengths.push_back(bf);
+    if (lengths.empty()) lengths.push_back(job->cfg.block_frames);
+    if (vpls.empty() || radices.empty()) return fail(KC_ERR_INVALID, "empty tuning space");
+    if ((vmask >> 2) || (rmask & ~0x7F0u)) return fail(KC_ERR_INVALID, "tuning mask names an unsupported value");
+    const uint32_t preroll = sp.preroll_blocks ? sp.preroll_blocks : 16;
+    const uint32_t timed = sp.timed_blocks ? sp.timed_blocks : 4;
+    std::vector<ks_tune_result> all;
+    for (uint32_t bf : lengths)
+        if (int rc = tune_block_length(*job, bf, vpls, radices, preroll, timed, all)) return rc;
+    size_t bi = 0;
+    for (size_t i = 1; i < all.size(); ++i)
+        if (all[i].voice_samples_per_s > all[bi].voice_samples_per_s) bi = i;
+    *best = job->cfg;
+    best->voices_per_lane = all[bi].voices_per_lane;
+    best->sort_radix_bits = all[bi].sort_radix_bits;
+    best->block_frames = all[bi].block_frames;
+    if (results)
+        for (size_t i = 0; i < all.size() && i < cap; ++i) results[i] = all[i];
+    if (n) *n = (uint32_t)all.size();
+    return KC_OK;
+}
 
 void ks_server_config_default(ks_server_config* c) {
     if (!c) return;
@@ -482,6 +686,29 @@ int ks_serve(const ks_server_config* cfg, const ks_job_spec* specs, uint32_t n_j
     if (cfg->max_jobs == 0 || cfg->max_jobs > 1024) return fail(KC_ERR_INVALID, "max_jobs must be in 1..=1024");
     std::memset(stats, 0, sizeof(*stats));
     if (n_jobs == 0) return KC_OK;
+    // With autotune, every job runs with the tunables that won on the job
+    // with the largest voice pool.
+    std::vector<ks_job_spec> tuned;
+    if (cfg->autotune) {
+        uint32_t big = 0;
+        for (uint32_t i = 1; i < n_jobs; ++i)
+            if (specs[i].cfg.max_voices > specs[big].cfg.max_voices) big = i;
+        ks_tune_space sp{};
+        sp.preroll_blocks = 8;
+        sp.timed_blocks = 3;
+        kc_config best{};
+        const auto t_tune = Clock::now();
+        if (int rc = ks_autotune(&specs[big], &sp, &best, nullptr, 0, nullptr)) return rc;
+        stats->tune_s = since(t_tune);
+        stats->tuned_voices_per_lane = best.voices_per_lane;
+        stats->tuned_sort_radix_bits = best.sort_radix_bits;
+        tuned.assign(specs, specs + n_jobs);
+        for (auto& t : tuned) {
+            t.cfg.voices_per_lane = best.voices_per_lane;
+            t.cfg.sort_radix_bits = best.sort_radix_bits;
+        }
+        specs = tuned.data();
+    }
     std::vector<Job> jobs(n_jobs);
     std::vector<uint32_t> order(n_jobs);
     for (uint32_t i = 0; i < n_jobs; ++i) {
@@ -494,7 +721,7 @@ int ks_serve(const ks_server_config* cfg, const ks_job_spec* specs, uint32_t n_j
         if (cfg->mode == KS_MODE_BATCHED && !same_batch_variant(specs[i].cfg, specs[0].cfg))
             return fail(KC_ERR_INVALID, "job " + std::to_string(i) +
                                             " differs from job 0 in device, block_frames, interpolation, "
-                                            "strict_fp, mix_mode or voices_per_lane");
+                                            "strict_fp, mix_mode, voices_per_lane or sort_radix_bits");
         if (specs[i].cfg.device != cfg->device)
             return fail(KC_ERR_INVALID, "job " + std::to_string(i) + " is configured for another device");
     }

@@ -53,19 +53,52 @@ __global__ void __launch_bounds__(256) k_compact_scatter(PoolArgs a, const uint3
 
 __global__ void k_commit(DevState* st, const uint32_t* total) { commit_body(st, total); }
 
+template <uint32_t RB>
 __global__ void __launch_bounds__(256) k_sort_count(PoolArgs a, SortLayout L, const uint32_t* keys,
                                                     uint32_t shift, uint32_t* counts) {
-    sort_count_body(a, L, keys, shift, counts, blockIdx.x, gridDim.x);
+    sort_count_body<RB>(a, L, keys, shift, counts, blockIdx.x, gridDim.x);
 }
 
+template <uint32_t RB>
 __global__ void __launch_bounds__(256) k_sort_scatter(PoolArgs a, SortLayout L, const uint32_t* keys_in,
                                                       const uint32_t* idx_in, uint32_t* keys_out,
                                                       uint32_t* idx_out, uint32_t shift,
                                                       const uint32_t* offsets) {
-    sort_scatter_body(a, L, keys_in, idx_in, keys_out, idx_out, shift, offsets, blockIdx.x, gridDim.x);
+    sort_scatter_body<RB>(a, L, keys_in, idx_in, keys_out, idx_out, shift, offsets, blockIdx.x, gridDim.x);
+}
+
+// One LSD pass of the pool sort at digit width RB: count, scan, scatter.
+template <uint32_t RB>
+void sort_pass(cudaStream_t q, uint32_t G, const PoolArgs& pa, const SortLayout& L, const uint32_t* kin,
+               const uint32_t* iin, uint32_t* kout, uint32_t* iout, uint32_t shift, uint32_t* counts,
+               uint32_t* total) {
+    k_sort_count<RB><<<G, 256, 0, q>>>(pa, L, kin, shift, counts);
+    k_scan_counts<<<1, 1024, 0, q>>>(counts, (1u << RB) * G, total);
+    k_sort_scatter<RB><<<G, 256, 0, q>>>(pa, L, kin, iin, kout, iout, shift, counts);
+}
+
+void sort_pass_rb(uint32_t rb, cudaStream_t q, uint32_t G, const PoolArgs& pa, const SortLayout& L,
+                  const uint32_t* kin, const uint32_t* iin, uint32_t* kout, uint32_t* iout, uint32_t shift,
+                  uint32_t* counts, uint32_t* total) {
+    switch (rb) {
+        case 4: sort_pass<4>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        case 5: sort_pass<5>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        case 6: sort_pass<6>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        case 7: sort_pass<7>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        case 9: sort_pass<9>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        case 10: sort_pass<10>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        default: sort_pass<8>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+    }
 }
 
 __global__ void __launch_bounds__(256) k_sort_gather(PoolArgs a, const uint32_t* idx) { sort_gather_body(a, idx, blockIdx.x, gridDim.x); }
+
+// The f32 copy of the sample pool: one conversion per sample, at creation.
+__global__ void __launch_bounds__(256) k_convert_pool(const int16_t* __restrict__ pcm, float* __restrict__ pcmf,
+                                                      uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        pcmf[i] = fmaxf(__fmul_rn((float)pcm[i], 1.0f / 32767.0f), -1.0f);
+}
 
 }  // namespace kc
 
@@ -96,6 +129,8 @@ uint32_t max_steal_of(const kc_config& c) {
 }
 
 uint32_t clz32(uint32_t v) { return v ? (uint32_t)__builtin_clz(v) : 32u; }
+
+uint32_t radix_of(const kc_config& c) { return c.sort_radix_bits ? c.sort_radix_bits : SORT_RADIX_DEFAULT; }
 
 // SortKeyLayout::plan, src/gpu/mod.rs:77-105.
 SortLayout plan_sort(uint32_t n_regions, uint32_t max_len) {
@@ -171,6 +206,7 @@ void free_all(kc_synth* s) {
     cudaFree(s->pool[0]);
     cudaFree(s->pool[1]);
     cudaFree(s->pcm);
+    cudaFree(s->pcmf);
     cudaFree(s->params);
     cudaFree(s->gates);
     cudaFree(s->chan);
@@ -216,6 +252,8 @@ int validate(const kc_config& c) {
         c.release_curve > 1 || c.mix_mode > 2)
         return fail(KC_ERR_INVALID, "unknown enum value in config");
     if (c.voices_per_lane > 2) return fail(KC_ERR_INVALID, "voices_per_lane must be 0, 1 or 2");
+    if (c.sort_radix_bits && (c.sort_radix_bits < SORT_RADIX_MIN || c.sort_radix_bits > SORT_RADIX_MAX))
+        return fail(KC_ERR_INVALID, "sort_radix_bits must be 0 or in 4..=10");
     if (c.max_param_variants == 0 || c.max_param_variants > 64)
         return fail(KC_ERR_INVALID, "max_param_variants must be in 1..=64");
     return KC_OK;
@@ -271,6 +309,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     ra.pool = pa.pool;
     ra.cap = s->cap;
     ra.pcm = s->pcm;
+    ra.pcmf = s->pcmf;
     ra.pcm_len = (uint32_t)std::min<uint64_t>(s->pcm_len, 0xFFFFFFFFull);
     ra.params = s->params;
     ra.params_per = s->params_per;
@@ -307,17 +346,15 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     if (!c.sort_voices) {
         k_compact_scatter<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
     } else {
-        const uint32_t passes = (s->sort.bits + 7) / 8;
+        const uint32_t passes = (s->sort.bits + s->radix - 1) / s->radix;
         const uint32_t G = s->compact_ctas;
         int cur = 0;
         for (uint32_t p = 0; p < passes; ++p) {
-            const uint32_t shift = 8 * p;
+            const uint32_t shift = s->radix * p;
             const uint32_t* kin = p == 0 ? nullptr : s->keys[cur];
             const uint32_t* iin = p == 0 ? nullptr : s->idx[cur];
-            k_sort_count<<<G, 256, 0, q>>>(pa, s->sort, kin, shift, s->counts);
-            k_scan_counts<<<1, 1024, 0, q>>>(s->counts, 256 * G, s->total + 1);
-            k_sort_scatter<<<G, 256, 0, q>>>(pa, s->sort, kin, iin, s->keys[cur ^ 1], s->idx[cur ^ 1], shift,
-                                             s->counts);
+            sort_pass_rb(s->radix, q, G, pa, s->sort, kin, iin, s->keys[cur ^ 1], s->idx[cur ^ 1], shift, s->counts,
+                         s->total + 1);
             cur ^= 1;
         }
         k_sort_gather<<<s->pool_ctas, 256, 0, q>>>(pa, s->idx[cur]);
@@ -350,7 +387,7 @@ uint32_t launches_per_block(const kc_synth* s) {
     n += 1 + 1 + 1;                                                       // spawn, render, reduce
     n += 3;                                                               // count, scan, commit
     if (!s->cfg.sort_voices) n += 1;
-    else n += 3 * ((s->sort.bits + 7) / 8) + 1;
+    else n += 3 * ((s->sort.bits + s->radix - 1) / s->radix) + 1;
     return n;
 }
 
@@ -360,13 +397,15 @@ uint64_t footprint(const kc_config& c, uint64_t cap, uint64_t pcm_len, uint64_t 
                    uint32_t tiles, uint32_t cmds_cap, uint32_t partial_slices, uint32_t compact_ctas) {
     const uint64_t samples = (uint64_t)c.block_frames * 2;
     uint64_t n = 2ull * VOICE_FIELDS * cap * 4;                                 // pool, double-buffered
-    n += std::max<uint64_t>(pcm_len, 1) * 2 + 64;                               // sample pool
+    n += std::max<uint64_t>(pcm_len, 1) * 2 + 64;                               // sample pool (i16)
+    n += std::max<uint64_t>(pcm_len, 1) * 4 + 64;                               // and its f32 copy
     n += params_per * sizeof(kc_region_params) * n_slots;                       // params variants
     n += (uint64_t)tiles * (KC_GATE_SLOTS + KC_BEND_CHANNELS * KC_CHAN_FIELDS) * 4;
     n += (uint64_t)cmds_cap * sizeof(kc_spawn_cmd) + samples * 4;               // spawn buffer, block
     n += (uint64_t)partial_slices * samples * (c.mix_mode == KC_MIX_F64 ? 8 : 4);
     if (c.mix_mode == KC_MIX_TWO_SUM) n += (uint64_t)partial_slices * samples * 4;
-    n += sizeof(DevState) + sizeof(BlockCtl) + SEL_ROUNDS * 256 * 4 + 256ull * compact_ctas * 4 + 16;
+    n += sizeof(DevState) + sizeof(BlockCtl) + SEL_ROUNDS * 256 * 4 + 16;
+    n += (uint64_t)std::max<uint32_t>(256u, 1u << radix_of(c)) * compact_ctas * 4;  // digit counts
     if (c.sort_voices) n += 4ull * cap * 4;                                     // keys, indices
     return n;
 }
@@ -455,6 +494,7 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
 
     s->cap = (uint32_t)((slots + 31) & ~31ull);
     s->vpl = cfg->voices_per_lane == 2 ? 2u : 1u;
+    s->radix = radix_of(*cfg);
     s->tiles = cfg->block_frames / cfg->gate_frames;
     s->params_per = params_len;
     s->n_slots = cfg->max_param_variants;
@@ -478,6 +518,12 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMalloc(&s->pool[1], pool_words * 4));
     KC_TRY(cudaMalloc(&s->pcm, std::max<uint64_t>(pool_len, 1) * 2 + 64));
     if (pool_len) KC_TRY(cudaMemcpy(s->pcm, pool, pool_len * 2, cudaMemcpyDefault));
+    KC_TRY(cudaMalloc(&s->pcmf, std::max<uint64_t>(pool_len, 1) * 4 + 64));
+    if (pool_len) {
+        k_convert_pool<<<(unsigned)std::min<uint64_t>((pool_len + 255) / 256, (uint64_t)s->sms * 16), 256, 0,
+                         s->stream>>>(s->pcm, s->pcmf, pool_len);
+        KC_TRY(cudaGetLastError());
+    }
     const size_t per_bytes = (size_t)params_len * sizeof(kc_region_params);
     KC_TRY(cudaMalloc(&s->params, per_bytes * s->n_slots));
     // Every slot starts as a copy of the bank's table, which is what
@@ -506,7 +552,7 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMemset(s->st, 0, sizeof(DevState)));
     KC_TRY(cudaMalloc(&s->ctl, sizeof(BlockCtl)));
     KC_TRY(cudaMalloc(&s->sel_hist, SEL_ROUNDS * 256 * 4));
-    KC_TRY(cudaMalloc(&s->counts, (size_t)256 * s->compact_ctas * 4));
+    KC_TRY(cudaMalloc(&s->counts, (size_t)std::max<uint32_t>(256u, 1u << s->radix) * s->compact_ctas * 4));
     KC_TRY(cudaMalloc(&s->total, 16));
     if (cfg->sort_voices) {
         for (int i = 0; i < 2; ++i) {
@@ -530,14 +576,26 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
 }
 
 int kc_synth_clone(kc_synth* src, kc_synth** out) {
-    if (!src || !out) return fail(KC_ERR_INVALID, "null argument");
+    if (!src) return fail(KC_ERR_INVALID, "null argument");
+    return kc_synth_clone_config(src, &src->cfg, out);
+}
+
+int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out) {
+    if (!src || !cfg || !out) return fail(KC_ERR_INVALID, "null argument");
     *out = nullptr;
+    // Only the tunables that change how a block is computed may differ.
+    kc_config a = src->cfg, b = *cfg;
+    a.voices_per_lane = b.voices_per_lane = 0;
+    a.sort_radix_bits = b.sort_radix_bits = 0;
+    if (std::memcmp(&a, &b, sizeof(a)) != 0)
+        return fail(KC_ERR_INVALID, "clone config may differ from the source only in voices_per_lane and "
+                                    "sort_radix_bits");
     cudaSetDevice(src->device);
     KC_CUDA(cudaStreamSynchronize(src->stream));
     kc_synth* s = nullptr;
     // The bank and variant-0 table come straight from the source's device
     // copies (cudaMemcpyDefault resolves device pointers under UVA).
-    if (int rc = kc_synth_create(&src->cfg, src->pcm, src->pcm_len, src->params, src->params_per,
+    if (int rc = kc_synth_create(cfg, src->pcm, src->pcm_len, src->params, src->params_per,
                                  src->n_regions, src->max_sample_len, &s))
         return rc;
     auto bail = [&](cudaError_t e) {
@@ -771,9 +829,11 @@ int kc_estimate_device_bytes(const kc_config* cfg, uint64_t pool_len, uint32_t p
     if (int rc = render_occupancy(*cfg, vpl, (size_t)RENDER_WARPS * SM_WARP * sizeof(float), &per_sm)) return rc;
     const uint64_t cap = (slots + 31) & ~31ull;
     const uint32_t render_warps = (uint32_t)(sms * per_sm) * RENDER_WARPS;
+    // The spawn buffer grows with the largest block; admission never hands a
+    // block more commands than the pool has slots.
     *bytes = footprint(*cfg, cap, pool_len, params_len, cfg->max_param_variants,
-                       cfg->block_frames / cfg->gate_frames, 4096, partial_slices_of(cap, vpl, render_warps),
-                       (uint32_t)sms * 2);
+                       cfg->block_frames / cfg->gate_frames, (uint32_t)std::max<uint64_t>(slots, 4096),
+                       partial_slices_of(cap, vpl, render_warps), (uint32_t)sms * 2);
     return KC_OK;
 }
 

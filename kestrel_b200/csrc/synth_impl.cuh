@@ -32,6 +32,7 @@ struct kc_synth {
     uint32_t* pool[2] = {nullptr, nullptr};
     int parity = 0;
     int16_t* pcm = nullptr;
+    float* pcmf = nullptr;      // the pool converted to f32 once (k_convert_pool)
     kc_region_params* params = nullptr;
     uint32_t* gates = nullptr;
     uint32_t* chan = nullptr;
@@ -52,6 +53,7 @@ struct kc_synth {
     uint32_t render_ctas = 0, render_warps = 0;
     uint32_t partial_slices = 0; // partial-mix slices allocated
     uint32_t vpl = 1;           // render voices per lane
+    uint32_t radix = 8;         // pool-sort digit width (bits)
     size_t render_smem = 0;
     uint32_t pool_ctas = 0;     // grid-stride passes
     uint32_t compact_ctas = 0;  // chunked passes (compaction, sort)

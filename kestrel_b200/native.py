@@ -58,7 +58,7 @@ class KcConfig(C.Structure):
         ("interpolation", C.c_uint32), ("decay_curve", C.c_uint32), ("release_curve", C.c_uint32),
         ("env_floor", C.c_float), ("sort_voices", C.c_uint32), ("max_param_variants", C.c_uint32),
         ("mix_mode", C.c_uint32), ("strict_fp", C.c_uint32), ("device", C.c_uint32),
-        ("voices_per_lane", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+        ("voices_per_lane", C.c_uint32), ("sort_radix_bits", C.c_uint32), ("reserved", C.c_uint32 * 5)]
 
 
 class KcBlockStats(C.Structure):
@@ -87,6 +87,7 @@ def default_config(**overrides) -> KcConfig:
     c.strict_fp = 1
     c.device = 0
     c.voices_per_lane = 0
+    c.sort_radix_bits = 0
     for k, v in overrides.items():
         if not hasattr(c, k):
             raise AttributeError(f"kc_config has no field {k!r}")
@@ -98,7 +99,8 @@ class KcBatchConfig(C.Structure):
     _fields_ = [
         ("device", C.c_uint32), ("max_jobs", C.c_uint32), ("block_frames", C.c_uint32),
         ("interpolation", C.c_uint32), ("strict_fp", C.c_uint32), ("mix_mode", C.c_uint32),
-        ("voices_per_lane", C.c_uint32), ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 8)]
+        ("voices_per_lane", C.c_uint32), ("use_graph", C.c_uint32), ("sort_radix_bits", C.c_uint32),
+        ("reserved", C.c_uint32 * 7)]
 
 
 def batch_config_for(cfg: KcConfig, max_jobs: int = 256, use_graph: bool = True) -> KcBatchConfig:
@@ -112,6 +114,7 @@ def batch_config_for(cfg: KcConfig, max_jobs: int = 256, use_graph: bool = True)
     b.mix_mode = cfg.mix_mode
     b.voices_per_lane = 2 if cfg.voices_per_lane == 2 else 1
     b.use_graph = 1 if use_graph else 0
+    b.sort_radix_bits = cfg.sort_radix_bits
     return b
 
 
@@ -124,6 +127,7 @@ CUDA_SYMBOLS = {
                                   C.c_uint32, C.POINTER(_P)]),
     "kc_synth_destroy": (None, [_P]),
     "kc_synth_clone": (C.c_int, [_P, C.POINTER(_P)]),
+    "kc_synth_clone_config": (C.c_int, [_P, C.POINTER(KcConfig), C.POINTER(_P)]),
     "kc_set_gates": (C.c_int, [_P, _P, C.c_size_t]),
     "kc_set_channels": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int]),
     "kc_set_params_variant": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t]),

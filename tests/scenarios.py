@@ -86,15 +86,19 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
                   n_params: int = 24, chan: bool = True, variants: int = 3, steal_rule=N.STEAL_QUIETEST,
                   admit_rule=N.ADMIT_LOUDEST, interpolation=N.INTERP_LINEAR, sort_voices: int = 0,
                   mix_mode=N.MIX_F32_TREE, strict_fp: int = 1, steal_percent: int = 25,
-                  release_rate: float = 0.3, unity_step: bool = False, decay_curve=N.CURVE_EXPONENTIAL,
-                  release_curve=N.CURVE_EXPONENTIAL, voices_per_lane: int = 0) -> Scenario:
+                  release_rate: float = 0.3, steps: str = "ratio", decay_curve=N.CURVE_EXPONENTIAL,
+                  release_curve=N.CURVE_EXPONENTIAL, voices_per_lane: int = 0, sort_radix_bits: int = 0) -> Scenario:
+    """steps: "ratio" (pitch ratios 2^U(-1.5, 1.5), random phase fractions),
+    "unit" (every step exactly 1.0 and every phase fraction zero: the root key
+    at the pool rate) or "integral" (steps of exactly 1, 2 or 3 with zero
+    phase fractions)."""
     rng = np.random.default_rng(seed)
     cfg = N.default_config(max_voices=max_voices, block_frames=block_frames, gate_frames=gate_frames,
                            steal_rule=steal_rule, admit_rule=admit_rule, interpolation=interpolation,
                            sort_voices=sort_voices, mix_mode=mix_mode, strict_fp=strict_fp,
                            max_steal_percent=steal_percent, max_param_variants=max(variants + 1, 1),
                            decay_curve=decay_curve, release_curve=release_curve,
-                           voices_per_lane=voices_per_lane)
+                           voices_per_lane=voices_per_lane, sort_radix_bits=sort_radix_bits)
     pool, starts, params = make_bank(rng, n_samples, frames, n_params)
     tiles = block_frames // gate_frames
     on_count = np.zeros(N.GATE_SLOTS, np.uint32)
@@ -120,8 +124,9 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
         start[edge] = length[edge] - 1
         cmds["phase_hi"] = start
         cmds["phase_lo"] = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
-        if unity_step:
-            cmds["step_hi"] = 1
+        if steps in ("unit", "integral"):
+            cmds["phase_lo"] = 0
+            cmds["step_hi"] = 1 if steps == "unit" else rng.integers(1, 4, n)
             cmds["step_lo"] = 0
         else:
             ratio = 2.0 ** rng.uniform(-1.5, 1.5, n)

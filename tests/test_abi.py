@@ -75,3 +75,23 @@ def test_create_without_device_fails_loudly():
     import numpy as np
     with pytest.raises(N.KestrelError):
         CudaSynth(N.default_config(max_voices=16), np.zeros(16, np.int16), np.zeros(1, N.PARAMS_DTYPE), 1, 16)
+
+
+def test_config_validation_needs_no_device():
+    """Invalid configs are refused before any device call (validation of the
+    tunables the autotuner sets included)."""
+    import numpy as np
+    lib = N.cuda_lib()
+    out = C.c_void_p()
+    pool = np.zeros(16, np.int16)
+    params = np.zeros(1, N.PARAMS_DTYPE)
+    for bad in (dict(sort_radix_bits=3), dict(sort_radix_bits=11), dict(voices_per_lane=3),
+                dict(block_frames=1000), dict(mix_mode=7)):
+        cfg = N.default_config(max_voices=16, **bad)
+        rc = lib.kc_synth_create(C.byref(cfg), N.ptr(pool), pool.size, N.ptr(params), 1, 1, 16, C.byref(out))
+        assert rc == 1, bad  # KC_ERR_INVALID
+        assert lib.kc_last_error()
+    b = N.KcBatchConfig()
+    lib.kc_batch_config_default(C.byref(b))
+    b.sort_radix_bits = 12
+    assert lib.kc_batch_create(C.byref(b), C.byref(out)) == 1

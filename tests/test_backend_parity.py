@@ -66,6 +66,45 @@ def test_parity_large_pool_sustained(vpl):
 
 
 @gpu
+@pytest.mark.parametrize("vpl", [1, 2])
+def test_parity_unit_steps(vpl):
+    """Every voice plays its sample at the root pitch (step exactly 1.0, zero
+    phase fractions), so sustained tiles take the fixed-offset path."""
+    sc = make_scenario(seed=14, max_voices=40000, n_blocks=4, spawn_per_block=(9000, 12000), release_rate=0.02,
+                       voices_per_lane=vpl, sort_voices=1, steps="unit", chan=False)
+    _compare(sc, sorted_pool=True)
+
+
+@gpu
+@pytest.mark.parametrize("interp", [N.INTERP_LINEAR, N.INTERP_NEAREST])
+def test_parity_integral_steps(interp):
+    """Whole-number steps (1, 2, 3) with zero phase fractions: the
+    zero-fraction paths for linear and nearest interpolation."""
+    sc = make_scenario(seed=15, max_voices=40000, n_blocks=4, spawn_per_block=(9000, 12000), release_rate=0.02,
+                       sort_voices=1, steps="integral", chan=False, interpolation=interp)
+    _compare(sc, sorted_pool=True)
+
+
+@gpu
+def test_sort_radix_widths_agree():
+    """The pool sort at every digit width leaves the same pool, so blocks
+    and pools are byte-identical to the default 8-bit width."""
+    from kestrel_b200.backend import CudaSynth
+    ref = None
+    for rb in (8, 4, 5, 7, 10):
+        sc = make_scenario(seed=16, max_voices=20000, n_blocks=4, spawn_per_block=(4000, 7000), sort_voices=1,
+                           sort_radix_bits=rb)
+        cu = CudaSynth(sc.cfg, sc.pool, sc.params, sc.n_regions, sc.max_len)
+        o, s, p, _ = run(cu, sc, collect_pool=True)
+        cu.close()
+        got = (np.concatenate(o).tobytes(), [x.tobytes() for x in p])
+        if ref is None:
+            ref = got
+        else:
+            assert got == ref, f"radix {rb}"
+
+
+@gpu
 def test_parity_oldest_even_nochan():
     sc = make_scenario(seed=2, steal_rule=N.STEAL_OLDEST, admit_rule=N.ADMIT_EVEN, chan=False, variants=0)
     _compare(sc)
