@@ -231,13 +231,15 @@ void* kc_stream(kc_synth* s);
 int kc_block_launches(kc_synth* s, uint32_t* out);
 
 /* ---- precision form ------------------------------------------------------ *
- * RBJ lowpass coefficients designed in FP64 on the device and rounded once to
- * f32: `coefs` receives n x (b0, b1, a1, a2) for the n (cutoff Hz, Q in
- * centibels) pairs, with the arithmetic of biquad_lowpass (src/bank.rs:
- * 956-979) carried out in double. For regions with a low cutoff or a high Q,
- * where the reference's f32 design loses most of (1 - cos w0); the caller
- * patches the returned coefficients into the params table it hands to
- * kc_synth_create / kc_set_params_variant. Host buffers in and out. */
+ * RBJ lowpass coefficients designed in FP64 on the device: `coefs` receives
+ * n x (b0, b1, a1, a2) for the n (cutoff Hz, Q in centibels) pairs, with the
+ * arithmetic of biquad_lowpass (src/bank.rs:956-979) carried out in double.
+ * a1 and a2 are the exact design rounded once to f32; b0 is matched to them
+ * (b0 = gain (1 + a1 + a2) / 4, b1 = 2 b0) so the stored filter keeps the
+ * design's DC gain to within one f32 rounding. For regions with a low cutoff
+ * or a high Q, where the reference's f32 design loses most of (1 - cos w0);
+ * the caller patches the returned coefficients into the params table it
+ * hands to kc_synth_create / kc_set_params_variant. Host buffers in and out. */
 int kc_design_lowpass_f64(const float* fc_hz, const float* q_cb, uint32_t n, float sample_rate,
                           float* coefs, int device);
 

@@ -7,8 +7,16 @@
 // a fraction of a dB; at high Q the poles sit within w0 / 2Q of the unit
 // circle, where that error also moves the resonance. Designing in FP64 and
 // rounding once to f32 leaves each coefficient within half an f32 ulp of the
-// exact design. This is the only FP64 arithmetic on the device; the render
-// recursion stays f32.
+// exact design. The numerator is then matched to the rounded denominator: in
+// exact arithmetic 1 + a1 + a2 = 2 (1 - cos w0) / a0 = 4 b0 / gain, so b0 is
+// taken as gain (1 + a1' + a2') / 4 from the f32-rounded a1', a2' (the sum is
+// exact in double) and b1 = 2 b0. The stored f32 filter then has the design's
+// DC gain to within one rounding of b0 (about -140 dB), where rounding each
+// coefficient on its own leaves the cancellation in 1 + a1' + a2' (0.06 dB at
+// 20 Hz). What no FP64 design removes is the f32 quantisation of a1 itself,
+// which moves a resonant pole at low cutoff by a fraction of its bandwidth.
+// This is the only FP64 arithmetic on the device; the render recursion stays
+// f32.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -40,8 +48,12 @@ __global__ void k_design_lowpass_f64(const float* __restrict__ fc_hz, const floa
     const double cos_w0 = cos(w0);
     const double alpha = sin(w0) / (2.0 * q);
     const double a0 = 1.0 + alpha;
-    out[i] = make_float4((float)(gain * one_minus_cos * 0.5 / a0), (float)(gain * one_minus_cos / a0),
-                         (float)(-2.0 * cos_w0 / a0), (float)((1.0 - alpha) / a0));
+    const float a1 = (float)(-2.0 * cos_w0 / a0);
+    const float a2 = (float)((1.0 - alpha) / a0);
+    // Numerator matched to the rounded poles (DC gain exactly `gain` but for
+    // b0's own rounding); b1 = 2 b0 is exact in f32.
+    const float b0 = (float)(gain * ((1.0 + (double)a1) + (double)a2) * 0.25);
+    out[i] = make_float4(b0, 2.0f * b0, a1, a2);
 }
 
 }  // namespace

@@ -38,7 +38,8 @@ struct RenderArgs {
     uint32_t* pool;            // current pool, field-major
     uint32_t cap;              // field stride in words
     const int16_t* pcm;        // sample pool, i16 as the bank holds it
-    const float* pcmf;         // the same pool converted once to f32 (F32 kernels)
+    const float* pcmf;         // the same pool converted once to f32 (F32 kernels), followed
+                               // by ZERO_PAD zero frames (the taps of neutral lanes)
     uint32_t pcm_len;          // frames in it
     const kc_region_params* params;  // n_slots copies of params_per
     uint32_t params_per;
@@ -56,6 +57,9 @@ struct RenderArgs {
     uint32_t exp_decay;
     uint32_t exp_release;
 };
+
+// Zero frames after the f32 pool: a neutral lane (below) reads its taps there.
+constexpr uint32_t ZERO_PAD = 32;
 
 // One in-bounds tap. The f32 pool holds exactly the value CpuSynth::fetch
 // (src/cpu.rs:187-194) computes from the i16 sample -- v / 32767 clamped at
@@ -107,7 +111,27 @@ struct VoiceRegs {
     bool loop_en, lur;
     uint32_t params_base, variant, born, born_gate;
     uint32_t slot, ordinal, start_rel, stop_rel, channel;
+    bool neutral;   // dead, and set to contribute exactly +0 on every path (neutralize)
 };
+
+// A voice that died (or a lane past the live count) keeps its lane idle for
+// the rest of the block, and an idle lane would keep the whole warp off the
+// hot paths. Instead the dead voice is made neutral: level, gains, filter
+// state and coefficients +0, taps at the zero pad after the f32 pool, step 0.
+// Every hot-path frame then computes +0 for it (all products are +0 * +0 and
+// all sums +0 + +0, whatever the path), and its phase never moves. Its stage
+// stays DEAD, so compaction drops it; nothing reads a dead voice's other
+// fields. Only kernels with the padded f32 pool (F32) do this.
+__device__ __forceinline__ void neutralize(VoiceRegs& v, const RenderArgs& a) {
+    v.level = 0.0f;
+    v.gl = v.gr = v.bgl = v.bgr = 0.0f;
+    v.z1 = v.z2 = 0.0f;
+    v.b0 = v.b1 = v.a1 = v.a2 = 0.0f;
+    v.base = a.pcm_len;
+    v.phase = 0;
+    v.step = v.base_step = 0;
+    v.neutral = true;
+}
 
 __device__ __forceinline__ void load_params(VoiceRegs& v, const RenderArgs& a, uint32_t variant) {
     const uint32_t s = variant < a.n_slots ? variant : 0u;
@@ -300,7 +324,8 @@ template <uint32_t NF>
 __device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a, uint32_t f0, bool looping,
                                         bool& active) {
     constexpr uint32_t LOG2 = NF == 32 ? 5 : 4;
-    active = false;
+    active = v.neutral;  // runs every path, contributing +0
+    if (v.neutral) return true;
     if (v.stage == ENV_DEAD || v.start_rel >= f0 + NF) return true;
     if (v.start_rel > f0) return false;                       // starts inside the span
     if (v.stop_rel != 0u && v.stop_rel <= f0 + NF) return false;  // fade begins inside
@@ -316,10 +341,9 @@ __device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a,
 }
 
 // The biquad (transposed direct form II, b2 == b0, src/cpu.rs:564-572) on one
-// sample; y = x when the region's filter is off.
+// sample.
 template <bool STRICT>
-__device__ __forceinline__ float biquad(VoiceRegs& v, float x) {
-    if (!v.filt) return x;
+__device__ __forceinline__ float biquad_core(VoiceRegs& v, float x) {
     float y;
     if (STRICT) {
         const float bx = __fmul_rn(v.b0, x);
@@ -332,6 +356,12 @@ __device__ __forceinline__ float biquad(VoiceRegs& v, float x) {
         v.z2 = fmaf(v.b0, x, -(v.a2 * y));
     }
     return y;
+}
+
+// y = x when the region's filter is off.
+template <bool STRICT>
+__device__ __forceinline__ float biquad(VoiceRegs& v, float x) {
+    return v.filt ? biquad_core<STRICT>(v, x) : x;
 }
 
 template <bool STRICT>
@@ -393,46 +423,6 @@ __device__ __forceinline__ bool level_at_most_one(const VoiceRegs& v, const EnvS
     return v.level <= 1.0f;
 }
 
-// A hot frame with a fractional phase: two taps and the lerp.
-template <bool STRICT, bool F32>
-__device__ __forceinline__ float hot_frame(VoiceRegs& v, const RenderArgs& a, const EnvStep& e) {
-    v.level = __fmaf_rn(v.level, e.em, e.ea);
-    const uint32_t i0 = v.base + (uint32_t)(v.phase >> 32);
-    const float s0 = tap<F32>(a, i0);
-    const float s1 = tap<F32>(a, i0 + 1u);
-    const float frac = __fmul_rn(__uint2float_rn((uint32_t)v.phase), 2.3283064365386963e-10f);
-    const float y = biquad<STRICT>(v, __fmul_rn(lerp<STRICT>(s0, s1, frac), v.level));
-    v.phase += v.step;
-    return y;
-}
-
-// A hot frame when every lane's phase and step have a zero fraction (an
-// exactly integer pitch ratio: the root key played at the pool rate, or whole
-// octaves of it). Then frac is 0 for every frame of the tile, and the linear
-// interpolation s0 + (s1 - s0) * 0 is exactly s0 (s0 is never -0: it is
-// v / 32767 clamped at -1, so +0 for a zero tap), in both the strict and the
-// fused form; nearest interpolation reads the same tap. The second tap, its
-// conversion and the lerp drop out, and the phase advances by the step's
-// integer part alone (`off` = base + phase_hi; the tile's phase is written
-// back once at its end).
-template <bool STRICT, bool F32>
-__device__ __forceinline__ float hot_frame_int(VoiceRegs& v, const RenderArgs& a, const EnvStep& e, uint32_t& off) {
-    v.level = __fmaf_rn(v.level, e.em, e.ea);
-    const float y = biquad<STRICT>(v, __fmul_rn(tap<F32>(a, off), v.level));
-    off += (uint32_t)(v.step >> 32);
-    return y;
-}
-
-// A hot frame of a voice whose step is exactly 1.0 (the sample played at its
-// root pitch at the pool rate -- every unbent note of a bank sampled per key):
-// frame i of the tile reads tap i past the tile's first, a fixed offset.
-template <bool STRICT, bool F32>
-__device__ __forceinline__ float hot_frame_unit(VoiceRegs& v, const RenderArgs& a, const EnvStep& e, uint32_t off0,
-                                                uint32_t i) {
-    v.level = __fmaf_rn(v.level, e.em, e.ea);
-    return biquad<STRICT>(v, __fmul_rn(tap<F32>(a, off0 + i), v.level));
-}
-
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
     s = __fadd_rn(a, b);
     const float bb = __fsub_rn(s, a);
@@ -462,6 +452,7 @@ __device__ __forceinline__ void load_voice(VoiceRegs& v, const RenderArgs& a, ui
     v.filt = false; v.loop_en = false; v.lur = false;
     v.params_base = 0; v.variant = 0; v.born = 0; v.born_gate = 0;
     v.slot = 0; v.ordinal = 0; v.start_rel = 0; v.stop_rel = 0; v.channel = 0;
+    v.neutral = false;
     if (!live) return;
     const uint32_t cap = a.cap;
     const uint32_t* P = a.pool + vi;
@@ -556,6 +547,10 @@ __device__ __forceinline__ void acc_out(float& yl, float& yr, float y, const Voi
 
 // The paths a tile can take, fastest first.
 constexpr int P_UNIT = 0, P_INT = 1, P_HOT = 2, P_FAST = 3, P_GENERAL = 4;
+// Filter mode of a hot tile, uniform over the warp: every lane's region
+// filters, none does, or it varies by lane (tested per frame). Neutral lanes
+// fit any mode (their coefficients and state are +0).
+constexpr int FM_NONE = 0, FM_ALL = 1, FM_LANE = 2;
 
 // Classify the NF frames from f0 for the whole warp: ok (linear: every lane
 // on the fast path), hot (no idle lane, no transition, level <= 1
@@ -564,7 +559,7 @@ constexpr int P_UNIT = 0, P_INT = 1, P_HOT = 2, P_FAST = 3, P_GENERAL = 4;
 // use. Warp-uniform result.
 template <int INTERP, int V, uint32_t NF>
 __device__ __forceinline__ int classify(const VoiceRegs (&v)[V], const RenderArgs& a, uint32_t f0, bool (&looping)[V],
-                                        bool (&active)[V], EnvStep (&e)[V]) {
+                                        bool (&active)[V], EnvStep (&e)[V], int& fm) {
     constexpr bool FASTPATHS = INTERP != KC_INTERP_CUBIC;
     bool ok = FASTPATHS;
 #pragma unroll
@@ -579,8 +574,15 @@ __device__ __forceinline__ int classify(const VoiceRegs (&v)[V], const RenderArg
         e[k] = env_constants(v[k], a);
         hot = hot && active[k] && no_transition<NF>(v[k], e[k]) && level_at_most_one(v[k], e[k]);
         integral = integral && ((uint32_t)v[k].phase | (uint32_t)v[k].step) == 0u;
-        unit = unit && v[k].step == (1ull << 32);
+        unit = unit && (v[k].neutral || v[k].step == (1ull << 32));
     }
+    bool all_f = true, no_f = true;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+        all_f = all_f && (v[k].neutral || v[k].filt);
+        no_f = no_f && (v[k].neutral || !v[k].filt);
+    }
+    fm = __all_sync(0xFFFFFFFFu, all_f) ? FM_ALL : (__all_sync(0xFFFFFFFFu, no_f) ? FM_NONE : FM_LANE);
     if (FASTPATHS && __all_sync(0xFFFFFFFFu, hot && integral && unit)) return P_UNIT;
     if (FASTPATHS && __all_sync(0xFFFFFFFFu, hot && integral)) return P_INT;
     if (INTERP == KC_INTERP_LINEAR && __all_sync(0xFFFFFFFFu, hot)) return P_HOT;
@@ -591,6 +593,116 @@ __device__ __forceinline__ int classify(const VoiceRegs (&v)[V], const RenderArg
 // This lane's (left, right) pair for frame i of the tile.
 __device__ __forceinline__ void put_pair(float* sm, uint32_t lane, uint32_t i, float yl, float yr) {
     *reinterpret_cast<float2*>(sm + i * SM_ROW + (lane >> 4) * SM_HALF + (lane & 15u) * 2u) = make_float2(yl, yr);
+}
+
+template <bool STRICT, int FM>
+__device__ __forceinline__ float biquad_fm(VoiceRegs& v, float x) {
+    if (FM == FM_NONE) return x;
+    if (FM == FM_LANE) return biquad<STRICT>(v, x);
+    return biquad_core<STRICT>(v, x);  // FM_ALL: no per-lane test
+}
+
+// Taps from a base index. The pointer is formed once, so a tap at a fixed
+// offset from it needs no address arithmetic of its own.
+template <bool F32>
+struct Taps {
+    const float* p = nullptr;
+    Taps() = default;
+    __device__ __forceinline__ Taps(const RenderArgs& a, uint32_t base) : p(a.pcmf + base) {}
+    __device__ __forceinline__ float operator[](uint32_t i) const { return __ldg(p + i); }
+};
+template <>
+struct Taps<false> {
+    const int16_t* p = nullptr;
+    Taps() = default;
+    __device__ __forceinline__ Taps(const RenderArgs& a, uint32_t base) : p(a.pcm + base) {}
+    __device__ __forceinline__ float operator[](uint32_t i) const {
+        return fmaxf(__fmul_rn((float)__ldg(p + i), 1.0f / 32767.0f), -1.0f);
+    }
+};
+
+// The hot tiles (no idle lane, no transition, level <= 1 throughout).
+//  P_UNIT  every step exactly 1.0 and every phase fraction zero (the sample at
+//          its root pitch at the pool rate -- every unbent note of a bank
+//          sampled per key): frame i reads tap i past the tile's first.
+//  P_INT   whole-number steps, zero fractions: frac is 0 on every frame, and
+//          the linear interpolation s0 + (s1 - s0) * 0 is exactly s0 (s0 is
+//          never -0: it is v / 32767 clamped at -1, so +0 for a zero tap), in
+//          both the strict and the fused form; nearest reads the same tap. The
+//          second tap and the lerp drop out and the phase advances by the
+//          step's integer part.
+//  P_HOT   fractional phases: two taps and the lerp, the 32.32 phase per frame.
+// fast_ok proved every tap in bounds and phase + 16 * step free of overflow,
+// so P_UNIT and P_INT write the phase back once at the end of the tile.
+template <int KIND, int FM, bool STRICT, bool F32, int V>
+__device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V], float* sm,
+                                         uint32_t lane) {
+    if constexpr (KIND == P_UNIT) {
+        Taps<F32> t[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) t[k] = Taps<F32>(a, v[k].base + (uint32_t)(v[k].phase >> 32));
+#pragma unroll
+        for (uint32_t i = 0; i < MIX_TILE; ++i) {
+            float yl, yr;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
+                const float y = biquad_fm<STRICT, FM>(v[k], __fmul_rn(t[k][i], v[k].level));
+                if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                else acc_out<STRICT, false>(yl, yr, y, v[k]);
+            }
+            put_pair(sm, lane, i, yl, yr);
+        }
+        // 16 frames of step 1.0 (a neutral lane's step is 0)
+#pragma unroll
+        for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
+    } else if constexpr (KIND == P_INT) {
+        uint32_t off[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
+#pragma unroll
+        for (uint32_t i = 0; i < MIX_TILE; ++i) {
+            float yl, yr;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
+                const float y = biquad_fm<STRICT, FM>(v[k], __fmul_rn(tap<F32>(a, off[k]), v[k].level));
+                off[k] += (uint32_t)(v[k].step >> 32);
+                if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                else acc_out<STRICT, false>(yl, yr, y, v[k]);
+            }
+            put_pair(sm, lane, i, yl, yr);
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
+    } else {
+#pragma unroll
+        for (uint32_t i = 0; i < MIX_TILE; ++i) {
+            float yl, yr;
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
+                const uint32_t i0 = v[k].base + (uint32_t)(v[k].phase >> 32);
+                const Taps<F32> t(a, i0);
+                const float frac = __fmul_rn(__uint2float_rn((uint32_t)v[k].phase), 2.3283064365386963e-10f);
+                const float y = biquad_fm<STRICT, FM>(v[k], __fmul_rn(lerp<STRICT>(t[0], t[1], frac), v[k].level));
+                v[k].phase += v[k].step;
+                if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
+                else acc_out<STRICT, false>(yl, yr, y, v[k]);
+            }
+            put_pair(sm, lane, i, yl, yr);
+        }
+    }
+}
+
+// Run a hot tile of kind `path` (P_UNIT, P_INT or, for linear
+// interpolation, P_HOT) with filter mode FM.
+template <int INTERP, int FM, bool STRICT, bool F32, int V>
+__device__ __forceinline__ void hot_dispatch(int path, VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V],
+                                             float* sm, uint32_t lane) {
+    if (path == P_UNIT) hot_tile<P_UNIT, FM, STRICT, F32, V>(v, a, e, sm, lane);
+    else if (path == P_INT) hot_tile<P_INT, FM, STRICT, F32, V>(v, a, e, sm, lane);
+    else if constexpr (INTERP == KC_INTERP_LINEAR) hot_tile<P_HOT, FM, STRICT, F32, V>(v, a, e, sm, lane);
 }
 
 // Render every batch of 32*V voices this warp owns. Lane l of batch b holds
@@ -626,7 +738,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
         // envelope constants, which no hot frame changes).
         EnvStep e[V];
         bool looping[V], active[V];
-        int carried = -1;
+        int carried = -1, fm = FM_LANE;
         uint32_t next_gate = 0, gt = 0;
         const bool span32 = a.gate_frames % 32u == 0u;
         for (uint32_t f0 = 0; f0 < a.block_frames; f0 += MIX_TILE) {
@@ -636,70 +748,32 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 ++gt;
                 next_gate += a.gate_frames;
             }
+            // This tile's word of the partial slice, fetched before the frames
+            // so its latency is spent rendering (f32 tree mix).
+            const uint32_t j = f0 * 2u + lane;
+            float part_prev = 0.0f;
+            if (MIX == KC_MIX_F32_TREE && !first) part_prev = part[j];
             int path;
             if (carried >= 0) {
                 path = carried;
                 carried = -1;
             } else {
+                if (F32) {
+#pragma unroll
+                    for (int k = 0; k < V; ++k)
+                        if (v[k].stage == ENV_DEAD && !v[k].neutral) neutralize(v[k], a);
+                }
                 path = P_GENERAL;
                 if (span32 && (f0 & 31u) == 0u) {
-                    path = classify<INTERP, V, 32>(v, a, f0, looping, active, e);
+                    path = classify<INTERP, V, 32>(v, a, f0, looping, active, e, fm);
                     if (path <= P_HOT) carried = path;
                 }
-                if (carried < 0) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e);
+                if (carried < 0) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e, fm);
             }
-            if (FASTPATHS && path == P_UNIT) {
-                // Unit steps, zero fractions: tap i of the tile is a fixed
-                // offset from the tile's first.
-                uint32_t off[V];
-#pragma unroll
-                for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
-#pragma unroll
-                for (uint32_t i = 0; i < MIX_TILE; ++i) {
-                    float yl, yr;
-#pragma unroll
-                    for (int k = 0; k < V; ++k) {
-                        const float y = hot_frame_unit<STRICT, F32>(v[k], a, e[k], off[k], i);
-                        if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
-                        else acc_out<STRICT, false>(yl, yr, y, v[k]);
-                    }
-                    put_pair(sm, lane, i, yl, yr);
-                }
-#pragma unroll
-                for (int k = 0; k < V; ++k) v[k].phase += (uint64_t)MIX_TILE << 32;
-            } else if (FASTPATHS && path == P_INT) {
-                // Straight-line frames with a zero phase fraction.
-                uint32_t off[V];
-#pragma unroll
-                for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
-#pragma unroll
-                for (uint32_t i = 0; i < MIX_TILE; ++i) {
-                    float yl, yr;
-#pragma unroll
-                    for (int k = 0; k < V; ++k) {
-                        const float y = hot_frame_int<STRICT, F32>(v[k], a, e[k], off[k]);
-                        if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
-                        else acc_out<STRICT, false>(yl, yr, y, v[k]);
-                    }
-                    put_pair(sm, lane, i, yl, yr);
-                }
-                // fast_ok proved phase + 16 * step does not overflow
-#pragma unroll
-                for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
-            } else if (INTERP == KC_INTERP_LINEAR && path == P_HOT) {
-                // Every lane's every voice is live for the whole tile with no
-                // stage change: straight-line code, no branches.
-#pragma unroll
-                for (uint32_t i = 0; i < MIX_TILE; ++i) {
-                    float yl, yr;
-#pragma unroll
-                    for (int k = 0; k < V; ++k) {
-                        const float y = hot_frame<STRICT, F32>(v[k], a, e[k]);
-                        if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
-                        else acc_out<STRICT, false>(yl, yr, y, v[k]);
-                    }
-                    put_pair(sm, lane, i, yl, yr);
-                }
+            if (path <= P_HOT) {
+                if (fm == FM_ALL) hot_dispatch<INTERP, FM_ALL, STRICT, F32, V>(path, v, a, e, sm, lane);
+                else if (fm == FM_NONE) hot_dispatch<INTERP, FM_NONE, STRICT, F32, V>(path, v, a, e, sm, lane);
+                else hot_dispatch<INTERP, FM_LANE, STRICT, F32, V>(path, v, a, e, sm, lane);
             } else if (INTERP == KC_INTERP_LINEAR && path == P_FAST) {
 #pragma unroll
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
@@ -733,7 +807,6 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
             __syncwarp();
             // Lane l owns output slot l of the tile: frame l >> 1, channel
             // l & 1, summed over the warp's 32 lanes.
-            const uint32_t j = f0 * 2u + lane;
             const uint32_t h = lane & 1u;
             const float* row = sm + (lane >> 1) * SM_ROW;
             if (MIX == KC_MIX_F32_TREE) {
@@ -761,7 +834,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 const float mine = h ? sr : sl;
                 const float theirs = __shfl_xor_sync(0xFFFFFFFFu, h ? sl : sr, 1);
                 const float sum = __fadd_rn(theirs, mine);  // (half 0) + (half 1) either way
-                part[j] = first ? sum : __fadd_rn(part[j], sum);
+                part[j] = first ? sum : __fadd_rn(part_prev, sum);
             } else {
                 // This lane's channel over all 32 lanes, in lane order.
                 float qq[32];

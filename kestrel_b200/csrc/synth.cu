@@ -398,7 +398,7 @@ uint64_t footprint(const kc_config& c, uint64_t cap, uint64_t pcm_len, uint64_t 
     const uint64_t samples = (uint64_t)c.block_frames * 2;
     uint64_t n = 2ull * VOICE_FIELDS * cap * 4;                                 // pool, double-buffered
     n += std::max<uint64_t>(pcm_len, 1) * 2 + 64;                               // sample pool (i16)
-    n += std::max<uint64_t>(pcm_len, 1) * 4 + 64;                               // and its f32 copy
+    n += (pcm_len + ZERO_PAD) * 4;                                               // its f32 copy + zero pad
     n += params_per * sizeof(kc_region_params) * n_slots;                       // params variants
     n += (uint64_t)tiles * (KC_GATE_SLOTS + KC_BEND_CHANNELS * KC_CHAN_FIELDS) * 4;
     n += (uint64_t)cmds_cap * sizeof(kc_spawn_cmd) + samples * 4;               // spawn buffer, block
@@ -518,7 +518,9 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMalloc(&s->pool[1], pool_words * 4));
     KC_TRY(cudaMalloc(&s->pcm, std::max<uint64_t>(pool_len, 1) * 2 + 64));
     if (pool_len) KC_TRY(cudaMemcpy(s->pcm, pool, pool_len * 2, cudaMemcpyDefault));
-    KC_TRY(cudaMalloc(&s->pcmf, std::max<uint64_t>(pool_len, 1) * 4 + 64));
+    // The f32 copy, then ZERO_PAD zero frames (neutral lanes' taps).
+    KC_TRY(cudaMalloc(&s->pcmf, (pool_len + ZERO_PAD) * 4));
+    KC_TRY(cudaMemsetAsync(s->pcmf + pool_len, 0, ZERO_PAD * 4, s->stream));
     if (pool_len) {
         k_convert_pool<<<(unsigned)std::min<uint64_t>((pool_len + 255) / 256, (uint64_t)s->sms * 16), 256, 0,
                          s->stream>>>(s->pcm, s->pcmf, pool_len);

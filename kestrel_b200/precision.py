@@ -41,9 +41,9 @@ def _db(x: float) -> float:
 def dense_mix(voices: int, blocks: int, seed: int = 1) -> list[dict]:
     cfg, bs, ms = H.config_workload("black", seed=seed)
     cfg.max_voices = voices
-    # Dense: about voices / 2 s of note-ons per second with 2 s notes, so the
-    # pool fills within a second and then stays full.
-    ms.notes = int(voices * 4)
+    # Dense: twice `voices` note-ons per second with 2 s notes, so the pool
+    # fills within about six blocks and then stays full.
+    ms.notes = int(voices * 16)
     ms.seconds = 8.0
     ms.dur_median_s = 2.0
     ms.dur_sigma = 0.5
@@ -160,7 +160,7 @@ def biquad_sweep(sr: float = 48000.0, seconds: float = 1.0, device: int = 0) -> 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--voices", type=int, default=4 * 1024 * 1024)
-    ap.add_argument("--blocks", type=int, default=6)
+    ap.add_argument("--blocks", type=int, default=10)
     ap.add_argument("--json", default=None)
     ap.add_argument("--skip-mix", action="store_true")
     args = ap.parse_args(argv)

@@ -185,10 +185,14 @@ def test_f64_mix_matches_the_oracle_f64_mix():
 
 @gpu
 def test_fp64_lowpass_design():
-    """kc_design_lowpass_f64 returns the exact RBJ design rounded once to f32.
-    The reference's f32 design agrees with it within the cancellation bound of
-    (1 - cos w0) in f32: a few ulp(1) / (1 - cos w0), relative, on b0 and b1
-    (about 1e-5 at 1 kHz, 50x that at 20 Hz)."""
+    """kc_design_lowpass_f64 designs the RBJ lowpass in double: the poles
+    (a1, a2) are the exact design rounded once to f32, and the numerator is
+    matched to those rounded poles, b0 = gain (1 + a1 + a2) / 4 and b1 = 2 b0,
+    so the stored f32 filter's DC gain is the design's to within b0's own
+    rounding (2^-24 relative). The reference's f32 design, rounded
+    coefficient by coefficient, misses the DC gain by the cancellation in
+    1 + a1 + a2 (hundreds of ulp at 20 Hz), which the check below shows
+    against the same bound."""
     from kestrel_b200 import host as H
     from kestrel_b200.precision import _design_exact
     lib = N.cuda_lib()
@@ -197,11 +201,15 @@ def test_fp64_lowpass_design():
     out = np.empty((fc.size, 4), np.float32)
     N.check(lib.kc_design_lowpass_f64(N.ptr(fc), N.ptr(q_cb), fc.size, 48000.0, N.ptr(out), 0), lib)
     exact = _design_exact(fc.astype(np.float64), q_cb.astype(np.float64), 48000.0)
-    rel = np.abs(out.astype(np.float64) - exact) / np.abs(exact)
-    assert np.all(rel <= 2.0 ** -23), rel
-    for i in (4, 5):
-        ref = np.array(H.biquad_lowpass(float(fc[i]), float(q_cb[i]), 48000.0), np.float64)
-        omc = 1.0 - np.cos(2 * np.pi * float(fc[i]) / 48000.0)
-        bound = 4 * 2.0 ** -24 / omc
-        assert np.all(np.abs(ref[:2] - out[i, :2]) / np.abs(out[i, :2]) <= bound), (i, ref, out[i])
-        assert np.all(np.abs(ref[2:] - out[i, 2:]) <= 8 * np.spacing(np.abs(out[i, 2:]))), (i, ref, out[i])
+    o = out.astype(np.float64)
+    # poles: the exact design rounded once
+    assert np.all(np.abs(o[:, 2:] - exact[:, 2:]) <= np.spacing(np.abs(out[:, 2:])) * 0.5), (o, exact)
+    # numerator: b1 = 2 b0 exactly, matched to the rounded poles
+    assert np.array_equal(out[:, 1], 2.0 * out[:, 0])
+    q = np.maximum(10.0 ** ((q_cb.astype(np.float64) / 10.0 - 3.01) / 20.0), 0.001)
+    gain = np.sqrt(np.sqrt(0.5) / q)
+    dc = (2 * o[:, 0] + o[:, 1]) / ((1 + o[:, 2]) + o[:, 3])
+    assert np.all(np.abs(dc / gain - 1) <= 2.0 ** -23), dc / gain - 1
+    ref = np.array([H.biquad_lowpass(float(f), float(c), 48000.0) for f, c in zip(fc, q_cb)], np.float64)
+    dc_ref = (2 * ref[:, 0] + ref[:, 1]) / ((1 + ref[:, 2]) + ref[:, 3])
+    assert np.abs(dc_ref[0] / gain[0] - 1) > 100 * 2.0 ** -23   # 20 Hz: the f32 design's DC drift
