@@ -721,7 +721,6 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
     // KC_MIX_F64: the same buffer holds one slice of doubles per warp.
     double* __restrict__ part_d = MIX == KC_MIX_F64 ? reinterpret_cast<double*>(a.partial) + (size_t)gw * samples
                                                     : nullptr;
-    constexpr bool FASTPATHS = INTERP != KC_INTERP_CUBIC;
 
     for (uint32_t b = gw; b < nbatch; b += tw) {
         VoiceRegs v[V];
