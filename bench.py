@@ -365,6 +365,17 @@ def run_served(args):
     return line
 
 
+def reduce_over_ranks(units, e2e_units, ms_t, e2e_s, device):
+    """Replicas: every rank rendered its own job. The job's work is the sum of
+    the ranks' voice-samples; its time is the slowest rank's."""
+    import torch
+    t = torch.tensor([float(units), float(e2e_units)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t)
+    m = torch.tensor([float(ms_t), float(e2e_s)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(m, op=torch.distributed.ReduceOp.MAX)
+    return float(t[0]), float(t[1]), float(m[0]), float(m[1])
+
+
 def workload_desc(name):
     return {
         "steal": "steal-saturation: 200M notes / 120 s, log-normal durations (median 6 s, sigma 0.5), "
@@ -421,13 +432,7 @@ def main(argv=None):
 
     units, ms_t, e2e_units, e2e_s = r["units"], r["ms"], r["e2e_units"], r["e2e_s"]
     if world > 1:
-        import torch
-        t = torch.tensor([float(units), float(e2e_units)], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t)
-        m = torch.tensor([ms_t, e2e_s], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(m, op=torch.distributed.ReduceOp.MAX)
-        units, e2e_units = float(t[0]), float(t[1])
-        ms_t, e2e_s = float(m[0]), float(m[1])
+        units, e2e_units, ms_t, e2e_s = reduce_over_ranks(units, e2e_units, ms_t, e2e_s, "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -3,7 +3,60 @@
 
 namespace kh {
 
-SynthMidi::SynthMidi(const kh_midi_spec& s) : spec_(s), rng_(s.seed) {
+void OffQueue::push(const Off& o) {
+    const uint64_t b = o.tick / w_;
+    ++size_;
+    if (buckets_.empty()) base_ = b;
+    if (b < base_) {
+        // Earlier than every bucket held (only before the first pop reaches
+        // it): open buckets down to it.
+        buckets_.insert(buckets_.begin(), base_ - b, std::vector<Off>());
+        base_ = b;
+        pos_ = 0;
+        front_sorted_ = false;
+    }
+    const uint64_t i = b - base_;
+    if (i >= buckets_.size()) buckets_.resize(i + 1);
+    std::vector<Off>& v = buckets_[i];
+    if (i == 0 && front_sorted_) {
+        // The bucket being consumed: keep its unconsumed part in order.
+        v.insert(std::upper_bound(v.begin() + pos_, v.end(), o), o);
+    } else {
+        v.push_back(o);
+    }
+}
+
+void OffQueue::settle() {
+    while (pos_ >= buckets_.front().size()) {
+        buckets_.pop_front();
+        ++base_;
+        pos_ = 0;
+        front_sorted_ = false;
+    }
+    if (!front_sorted_) {
+        std::sort(buckets_.front().begin(), buckets_.front().end());
+        front_sorted_ = true;
+    }
+}
+
+const OffQueue::Off& OffQueue::top() {
+    settle();
+    return buckets_.front()[pos_];
+}
+
+void OffQueue::pop() {
+    settle();
+    ++pos_;
+    --size_;
+    if (size_ == 0) {
+        buckets_.clear();
+        pos_ = 0;
+        front_sorted_ = false;
+    }
+}
+
+SynthMidi::SynthMidi(const kh_midi_spec& s)
+    : spec_(s), rng_(s.seed), offs_((uint64_t)std::max(1.0, 2.0 * (double)(s.ppq ? s.ppq : 9600) / 1000.0)) {
     if (spec_.ppq == 0) spec_.ppq = 9600;
     // 120 bpm: two quarter notes per second.
     ticks_per_s_ = 2.0 * (double)spec_.ppq;
@@ -162,7 +215,7 @@ bool SynthMidi::next(uint64_t* tick, Event* ev) {
     ev->b = o.vel;
     uint64_t off = tick_of((double)o.tick / ticks_per_s_ + o.dur_s);
     if (off <= o.tick) off = o.tick + 1;
-    offs_.push(Off{off, off_seq_++, o.ch, o.key});
+    offs_.push(Off{off, off_seq_++, o.ch, o.key});  // (tick, seq) order, as pops return them
     return true;
 }
 

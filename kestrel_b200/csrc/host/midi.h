@@ -5,7 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
-#include <queue>
+#include <deque>
 #include <random>
 #include <vector>
 
@@ -45,9 +45,39 @@ struct TempoClock {
     double frame_at(uint64_t tick) const { return base_frame + (double)(tick - base_tick) * frames_per_tick; }
 };
 
+// Pending note-offs, popped in (tick, seq) order. A calendar queue: one
+// unsorted bucket per BUCKET ticks, and the bucket being consumed sorted once
+// when it is reached. Pushes append (an off landing in the bucket being
+// consumed is inserted in order), so a stream holding millions of pending
+// offs costs a sort of each ~1 ms bucket instead of a heap operation with a
+// cache miss per level for every note.
+class OffQueue {
+   public:
+    struct Off {
+        uint64_t tick, seq;
+        uint8_t ch, key;
+        bool operator<(const Off& o) const { return tick != o.tick ? tick < o.tick : seq < o.seq; }
+    };
+    explicit OffQueue(uint64_t bucket_ticks) : w_(bucket_ticks ? bucket_ticks : 1) {}
+    bool empty() const { return size_ == 0; }
+    void push(const Off& o);
+    // The smallest pending off; only when !empty().
+    const Off& top();
+    void pop();
+
+   private:
+    void settle();  // make buckets_.front() the first non-empty bucket, sorted
+    uint64_t w_;
+    std::deque<std::vector<Off>> buckets_;  // bucket base_ + i
+    uint64_t base_ = 0;
+    size_t pos_ = 0;                        // consumed prefix of buckets_.front()
+    bool front_sorted_ = false;
+    size_t size_ = 0;
+};
+
 // The synthetic stream. Onsets are generated one window of time at a time:
 // background notes as a Poisson process, plus (optionally) 1 ms clusters of
-// many simultaneous notes; every onset schedules its note-off in a min-heap.
+// many simultaneous notes; every onset schedules its note-off in an OffQueue.
 // Controller curves and program changes run on their own schedule. The three
 // sources are merged by tick (at equal ticks: offs, then controllers, then
 // ons), so the stream is a pure function of the spec.
@@ -59,11 +89,7 @@ class SynthMidi {
     uint32_t ppq() const { return spec_.ppq; }
 
    private:
-    struct Off {
-        uint64_t tick, seq;
-        uint8_t ch, key;
-        bool operator>(const Off& o) const { return tick != o.tick ? tick > o.tick : seq > o.seq; }
-    };
+    using Off = OffQueue::Off;
     struct On {
         uint64_t tick;
         uint8_t ch, key, vel;
@@ -80,7 +106,7 @@ class SynthMidi {
     uint64_t onsets_made_ = 0;
     std::vector<On> ons_;
     size_t on_pos_ = 0;
-    std::priority_queue<Off, std::vector<Off>, std::greater<Off>> offs_;
+    OffQueue offs_;
     uint64_t off_seq_ = 0;
     // controller schedule
     uint64_t ctrl_step_ = 0;            // index of the next controller time step
