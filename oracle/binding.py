@@ -27,6 +27,7 @@ ORACLE_SYMBOLS = {
     "ko_render": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_int]),
     "ko_stats": (C.c_int, [_P, C.POINTER(N.KcBlockStats)]),
     "ko_read_pool": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_uint32)]),
+    "ko_load_pool": (C.c_int, [_P, _P, C.c_uint32, C.c_uint64, C.c_uint64]),
     "ko_max_steal": (C.c_uint32, [C.POINTER(N.KcConfig)]),
     "ko_steal_span": (C.c_uint32, [C.POINTER(N.KcConfig)]),
     "ko_pool_slots": (C.c_uint32, [C.POINTER(N.KcConfig)]),
@@ -119,3 +120,10 @@ class OracleSynth:
         assert self._lib.ko_read_pool(self._h, N.ptr(buf), buf.size, C.byref(live)) == 0
         n = live.value
         return buf[: 24 * n].reshape(24, n).copy()
+
+    def load_pool(self, fields: np.ndarray, stolen: int, dropped: int) -> None:
+        """Take over a pool read from another backend ([24, live] u32, the
+        kc_read_pool layout) with its cumulative counters."""
+        f = np.ascontiguousarray(fields, dtype=np.uint32)
+        assert f.ndim == 2 and f.shape[0] == 24
+        assert self._lib.ko_load_pool(self._h, N.ptr(f) if f.size else None, f.shape[1], stolen, dropped) == 0

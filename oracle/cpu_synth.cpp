@@ -591,4 +591,44 @@ int ko_read_pool(const ko_synth* s, uint32_t* fields, size_t cap_words, uint32_t
     return KC_OK;
 }
 
+int ko_load_pool(ko_synth* s, const uint32_t* fields, uint32_t live, uint64_t stolen, uint64_t dropped) {
+    if (!s || (live && !fields)) return KC_ERR_INVALID;
+    Pool p;
+    const size_t n = live;
+    auto col = [&](int f, size_t i) { return fields[(size_t)f * n + i]; };
+    auto colf = [&](int f, size_t i) {
+        float x;
+        const uint32_t w = col(f, i);
+        std::memcpy(&x, &w, 4);
+        return x;
+    };
+    for (size_t i = 0; i < n; ++i) {
+        p.phase.push_back(((uint64_t)col(1, i) << 32) | col(0, i));
+        p.step.push_back(((uint64_t)col(3, i) << 32) | col(2, i));
+        p.smp_base.push_back(col(4, i));
+        p.smp_len.push_back(col(5, i));
+        p.loop_start.push_back(col(6, i));
+        p.loop_end.push_back(col(7, i));
+        p.flags.push_back(col(8, i));
+        p.env_stage.push_back(col(9, i));
+        p.env_level.push_back(colf(10, i));
+        p.gain_l.push_back(colf(11, i));
+        p.gain_r.push_back(colf(12, i));
+        p.filt_z1.push_back(colf(13, i));
+        p.filt_z2.push_back(colf(14, i));
+        p.params.push_back(col(15, i));
+        p.region.push_back(col(16, i));
+        p.gate_slot.push_back(col(17, i));
+        p.ordinal.push_back(col(18, i));
+        p.start_rel.push_back(col(19, i));
+        p.note_id.push_back(((uint64_t)col(21, i) << 32) | col(20, i));
+        p.born_variant.push_back(col(22, i));
+        p.stop_rel.push_back(col(23, i));
+    }
+    s->pool = std::move(p);
+    s->stolen = stolen;
+    s->dropped = dropped;
+    return KC_OK;
+}
+
 }  // extern "C"

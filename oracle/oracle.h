@@ -47,6 +47,11 @@ int ko_render(ko_synth* s, float* out, size_t n, double* mix64, int threads);
 int ko_stats(const ko_synth* s, kc_block_stats* out);
 /* Same layout as kc_read_pool: 24 fields, field-major, stride *live. */
 int ko_read_pool(const ko_synth* s, uint32_t* fields, size_t cap_words, uint32_t* live);
+/* Replace the pool with `live` voices in that layout (a pool read from
+ * another backend between blocks) and set the cumulative counters. Lets a
+ * test hand a device context's steady state to the oracle and compare the
+ * next block at full size. */
+int ko_load_pool(ko_synth* s, const uint32_t* fields, uint32_t live, uint64_t stolen, uint64_t dropped);
 
 /* config.rs arithmetic, restated for the tests. */
 uint32_t ko_max_steal(const kc_config* cfg);
