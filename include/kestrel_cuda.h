@@ -243,6 +243,20 @@ int kc_block_launches(kc_synth* s, uint32_t* out);
 int kc_design_lowpass_f64(const float* fc_hz, const float* q_cb, uint32_t n, float sample_rate,
                           float* coefs, int device);
 
+/* ---- load-time resampling -------------------------------------------------- *
+ * SincBank::process (src/resample.rs:51-107) for a batch of samples in one
+ * launch, bit-exact with the host loop: source i (src_len[i] frames) at
+ * ratio[i] (output rate / input rate) goes to dst[i], which must hold
+ * dst_len[i] = max(round(src_len[i] * ratio[i]), 1) frames; table[i] is that
+ * ratio's 512 x 32 f32 sinc table (kh_sinc_table), built on the host so no
+ * device transcendental enters the result. `device` points to the CUDA ordinal
+ * (NULL: device 0). Host buffers in and out. The signature is the host
+ * library's kh_resample_fn, so kh_set_resampler(kc_resample_i16_batch, &ord)
+ * moves every bank's load-time conversion onto the GPU. */
+int kc_resample_i16_batch(void* device, uint32_t n, const int16_t* const* src, const uint32_t* src_len,
+                          const double* ratio, const float* const* table, int16_t* const* dst,
+                          const uint32_t* dst_len);
+
 /* ---- rendering without allocating --------------------------------------- *
  * No counterpart in the reference. For callers that cannot call cudaMalloc:
  * allocation can synchronise the whole device and take milliseconds, which a

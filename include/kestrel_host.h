@@ -184,6 +184,23 @@ float kh_timecents_to_secs(float tc);
 /* resample::resample_i16; `out` holds at least round(n * ratio) + 1 samples.
  * Returns the output length. */
 size_t kh_resample_i16(const int16_t* src, size_t n, double ratio, int16_t* out, size_t cap);
+
+/* A batch resampler the bank builder hands every sample it converts at load
+ * (build_pool, src/sf2.rs:585-703) instead of running the host loop, e.g.
+ * kc_resample_i16_batch on a GPU. Source i (src_len[i] frames) at ratio[i]
+ * goes to dst[i], which holds dst_len[i] = max(round(src_len[i] * ratio[i]),
+ * 1) frames; table[i] is that ratio's 512 x 32 f32 sinc table, phase-major,
+ * built by the host (SincBank::new, src/resample.rs:18-49). It must produce
+ * the host loop's output bit for bit. Returns 0 on success; on failure the
+ * bank falls back to the host loop. */
+typedef int (*kh_resample_fn)(void* user, uint32_t n, const int16_t* const* src, const uint32_t* src_len,
+                              const double* ratio, const float* const* table, int16_t* const* dst,
+                              const uint32_t* dst_len);
+/* Install (or, with fn = NULL, remove) the process-wide resampler. Set it
+ * before banks are built; banks built concurrently may share it. */
+void kh_set_resampler(kh_resample_fn fn, void* user);
+/* The sinc table the host builds for a ratio: PHASES x TAPS = 512 x 32 f32. */
+int kh_sinc_table(double ratio, float* out, size_t cap);
 uint64_t kh_mix48(uint64_t index);
 uint64_t kh_rank_gain_q(float gain_l, float gain_r);
 

@@ -67,7 +67,9 @@ typedef struct ks_server_config {
     uint32_t autotune;           /* 1: before serving, run ks_autotune (voices per lane, sort digit
                                     width) on the job with the largest voice pool and give every
                                     job the winner */
-    uint32_t reserved[7];
+    uint32_t device_resample;    /* 1 (default): banks built during the run convert their samples
+                                    on the server's GPU (kc_resample_i16_batch); 0: host loop */
+    uint32_t reserved[6];
 } ks_server_config;
 
 typedef struct ks_job_result {

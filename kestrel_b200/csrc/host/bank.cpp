@@ -4,9 +4,11 @@
 #include "bank.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <set>
+#include <unordered_map>
 
 namespace kh {
 
@@ -393,6 +395,8 @@ double sinc(double x) {
     return std::sin(px) / px;
 }
 
+}  // namespace
+
 // SincBank::new, src/resample.rs:15-49.
 std::vector<float> sinc_table(double ratio) {
     const double cutoff = (ratio < 1.0 ? ratio : 1.0) * 0.95;
@@ -418,7 +422,23 @@ std::vector<float> sinc_table(double ratio) {
     }
     return table;
 }
+
+namespace {
+std::atomic<kh_resample_fn> g_resample_fn{nullptr};
+std::atomic<void*> g_resample_user{nullptr};
 }  // namespace
+
+void set_resample_hook(kh_resample_fn fn, void* user) {
+    g_resample_user.store(user);
+    g_resample_fn.store(fn);
+}
+
+ResampleHook resample_hook() {
+    ResampleHook h;
+    h.fn = g_resample_fn.load();
+    h.user = g_resample_user.load();
+    return h;
+}
 
 // SincBank::process + resample_i16, src/resample.rs:51-107.
 std::vector<int16_t> resample_i16(const std::vector<int16_t>& src, double ratio) {
@@ -642,6 +662,41 @@ bool load_sf2(const Sf2& sf, const BankConfig& cfg, Bank* bank, std::string* err
     std::vector<uint32_t> remap(sf.samples.size(), UINT32_MAX);
     Bank& b = *bank;
     b = Bank{};
+    // With a batch resampler installed, every sample that needs converting
+    // goes to it in one call (one sinc table per distinct ratio).
+    std::unordered_map<uint32_t, std::vector<int16_t>> converted;
+    if (const ResampleHook hook = resample_hook(); hook.fn && pool_rate != 0) {
+        std::vector<uint32_t> ids, src_len, dst_len;
+        std::vector<const int16_t*> src;
+        std::vector<double> ratios;
+        std::vector<const float*> tabs;
+        std::vector<int16_t*> dst;
+        std::unordered_map<uint64_t, std::vector<float>> tables;  // by the ratio's bits
+        for (uint32_t sid : used) {
+            const Sf2Sample& sh = sf.samples[sid];
+            const uint32_t src_rate = std::max<uint32_t>(sh.rate, 1);
+            if (pool_rate == src_rate || sh.data.empty()) continue;
+            const double ratio = (double)pool_rate / (double)src_rate;
+            if (std::fabs(ratio - 1.0) < 1e-12) continue;
+            uint64_t key;
+            std::memcpy(&key, &ratio, 8);
+            auto it = tables.find(key);
+            if (it == tables.end()) it = tables.emplace(key, sinc_table(ratio)).first;
+            const size_t out_len = std::max<size_t>(sat_cast<size_t>(std::round((double)sh.data.size() * ratio)), 1);
+            auto& out = converted[sid];
+            out.resize(out_len);
+            ids.push_back(sid);
+            src.push_back(sh.data.data());
+            src_len.push_back((uint32_t)sh.data.size());
+            ratios.push_back(ratio);
+            tabs.push_back(it->second.data());
+            dst.push_back(out.data());
+            dst_len.push_back((uint32_t)out_len);
+        }
+        if (!ids.empty() && hook.fn(hook.user, (uint32_t)ids.size(), src.data(), src_len.data(), ratios.data(),
+                                    tabs.data(), dst.data(), dst_len.data()) != 0)
+            converted.clear();  // the host loop below converts them instead
+    }
     for (uint32_t sid : used) {
         const Sf2Sample& sh = sf.samples[sid];
         const uint32_t src_rate = std::max<uint32_t>(sh.rate, 1);
@@ -649,7 +704,8 @@ bool load_sf2(const Sf2& sf, const BankConfig& cfg, Bank* bank, std::string* err
         std::vector<int16_t> data;
         if (pool_rate != 0 && pool_rate != src_rate) {
             const double ratio = (double)pool_rate / (double)src_rate;
-            data = resample_i16(sh.data, ratio);
+            if (auto it = converted.find(sid); it != converted.end()) data = std::move(it->second);
+            else data = resample_i16(sh.data, ratio);
             loop_start = sat_cast<uint32_t>(std::round((double)loop_start * ratio));
             loop_end = sat_cast<uint32_t>(std::round((double)loop_end * ratio));
         } else {

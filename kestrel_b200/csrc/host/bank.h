@@ -153,6 +153,15 @@ bool load_sf2(const Sf2& sf, const BankConfig& cfg, Bank* out, std::string* err)
 
 // resample::resample_i16 (src/resample.rs:102-107).
 std::vector<int16_t> resample_i16(const std::vector<int16_t>& src, double ratio);
+// SincBank::new (src/resample.rs:18-49): 512 phases x 32 taps, phase-major.
+std::vector<float> sinc_table(double ratio);
+// The batch resampler kh_set_resampler installed, or null.
+struct ResampleHook {
+    kh_resample_fn fn = nullptr;
+    void* user = nullptr;
+};
+ResampleHook resample_hook();
+void set_resample_hook(kh_resample_fn fn, void* user);
 
 // testkit waveforms (src/testkit.rs:19-53).
 std::vector<int16_t> noise(size_t n, uint64_t seed);

@@ -828,6 +828,16 @@ size_t kh_resample_i16(const int16_t* src, size_t n, double ratio, int16_t* out,
     std::memcpy(out, r.data(), m * 2);
     return r.size();
 }
+void kh_set_resampler(kh_resample_fn fn, void* user) { set_resample_hook(fn, user); }
+int kh_sinc_table(double ratio, float* out, size_t cap) {
+    const std::vector<float> t = sinc_table(ratio);
+    if (!out || cap < t.size()) {
+        g_err = "sinc table: need 512 * 32 floats";
+        return 1;
+    }
+    std::memcpy(out, t.data(), t.size() * 4);
+    return 0;
+}
 uint64_t kh_mix48(uint64_t index) { return mix48(index); }
 uint64_t kh_rank_gain_q(float gain_l, float gain_r) { return rank_gain_q(gain_l, gain_r); }
 

@@ -154,7 +154,8 @@ void release(Job& j) {
     j.bank = nullptr;
 }
 
-// Bank and driver: host work only.
+// Bank and driver (the bank's samples convert on the GPU when the server
+// installed the device resampler).
 void setup(Job& j) {
     const auto t0 = Clock::now();
     const ks_job_spec& sp = *j.spec;
@@ -660,6 +661,7 @@ void ks_server_config_default(ks_server_config* c) {
     c->vram_budget = 0;
     c->use_graph = 1;
     c->realtime_arrivals = 1;
+    c->device_resample = 1;
 }
 
 uint64_t ks_hash_block(uint64_t h, const float* out, size_t n) {
@@ -727,9 +729,13 @@ int ks_serve(const ks_server_config* cfg, const ks_job_spec* specs, uint32_t n_j
     }
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t a, uint32_t b) { return specs[a].arrival_s < specs[b].arrival_s; });
+    // Banks built during the run convert their samples on the server's GPU.
+    int resample_device = (int)cfg->device;
+    if (cfg->device_resample) kh_set_resampler(kc_resample_i16_batch, &resample_device);
     const auto t0 = Clock::now();
     const int rc = cfg->mode == KS_MODE_SEQUENTIAL ? serve_sequential(*cfg, jobs, order, *stats, t0)
                                                    : serve_batched(*cfg, jobs, order, *stats, t0);
+    if (cfg->device_resample) kh_set_resampler(nullptr, nullptr);
     stats->wall_s = since(t0);
     for (uint32_t i = 0; i < n_jobs; ++i) {
         stats->voice_samples += results[i].voice_samples;

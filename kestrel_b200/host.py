@@ -85,6 +85,8 @@ HOST_SYMBOLS = {
                                  C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "kh_timecents_to_secs": (C.c_float, [C.c_float]),
     "kh_resample_i16": (C.c_size_t, [_P, C.c_size_t, C.c_double, _P, C.c_size_t]),
+    "kh_set_resampler": (None, [_P, _P]),
+    "kh_sinc_table": (C.c_int, [C.c_double, _P, C.c_size_t]),
     "kh_mix48": (C.c_uint64, [C.c_uint64]),
     "kh_rank_gain_q": (C.c_uint64, [C.c_float, C.c_float]),
 }
@@ -165,6 +167,28 @@ def resample_i16(src: np.ndarray, ratio: float) -> np.ndarray:
     out = np.empty(cap, np.int16)
     n = lib().kh_resample_i16(N.ptr(src), src.size, ratio, N.ptr(out), cap)
     return out[:n].copy()
+
+
+def sinc_table(ratio: float) -> np.ndarray:
+    """SincBank::new's 512 x 32 f32 table for a ratio (phase-major)."""
+    t = np.empty(512 * 32, np.float32)
+    if lib().kh_sinc_table(ratio, N.ptr(t), t.size) != 0:
+        raise RuntimeError(lib().kh_last_error().decode())
+    return t.reshape(512, 32)
+
+
+_device_ordinals: dict = {}
+
+
+def use_device_resampler(device: int | None = 0) -> None:
+    """Route every bank's load-time resampling through kc_resample_i16_batch
+    on `device` (None: back to the host loop). Process-wide."""
+    if device is None:
+        lib().kh_set_resampler(None, None)
+        return
+    cuda = N.cuda_lib()
+    ordinal = _device_ordinals.setdefault(device, C.c_int(device))  # kept alive for the hook
+    lib().kh_set_resampler(C.cast(cuda.kc_resample_i16_batch, C.c_void_p), C.cast(C.byref(ordinal), C.c_void_p))
 
 
 def mix48(i: int) -> int:

@@ -146,6 +146,7 @@ CUDA_SYMBOLS = {
     "kc_block_launches": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "kc_read_pool": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_uint32)]),
     "kc_design_lowpass_f64": (C.c_int, [_P, _P, C.c_uint32, C.c_float, _P, C.c_int]),
+    "kc_resample_i16_batch": (C.c_int, [_P, C.c_uint32, _P, _P, _P, _P, _P, _P]),
     "kc_batch_config_default": (C.c_int, [C.POINTER(KcBatchConfig)]),
     "kc_batch_create": (C.c_int, [C.POINTER(KcBatchConfig), C.POINTER(_P)]),
     "kc_batch_destroy": (None, [_P]),

@@ -37,7 +37,7 @@ class KsServerConfig(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("device", C.c_uint32), ("max_jobs", C.c_uint32),
                 ("host_threads", C.c_uint32), ("vram_budget", C.c_uint64), ("use_graph", C.c_uint32),
                 ("realtime_arrivals", C.c_uint32), ("on_block", BLOCK_FN), ("user", C.c_void_p),
-                ("autotune", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+                ("autotune", C.c_uint32), ("device_resample", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 class KsJobResult(C.Structure):
@@ -154,7 +154,7 @@ def autotune(job: JobSpec, voices_per_lane=(1, 2), radix_bits=(6, 8, 10), block_
 
 def serve(jobs: list[JobSpec], mode: int = MODE_BATCHED, device: int = 0, max_jobs: int = 256,
           host_threads: int = 0, vram_budget: int = 0, use_graph: bool = True, realtime_arrivals: bool = True,
-          on_block=None, autotune: bool = False) -> RunResult:
+          on_block=None, autotune: bool = False, device_resample: bool = True) -> RunResult:
     """Run every job to completion; raises on a failure that stopped the
     server (a job's own failure is its result's `status`).
 
@@ -171,6 +171,7 @@ def serve(jobs: list[JobSpec], mode: int = MODE_BATCHED, device: int = 0, max_jo
     sc.use_graph = 1 if use_graph else 0
     sc.realtime_arrivals = 1 if realtime_arrivals else 0
     sc.autotune = 1 if autotune else 0
+    sc.device_resample = 1 if device_resample else 0
     cb = None
     if on_block is not None:
         def _cb(_user, job, block, out, n):

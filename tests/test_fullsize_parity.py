@@ -50,10 +50,16 @@ def test_steal_saturation_block_at_full_size():
     bank = H.Bank(bs, cfg)
     drv = H.Driver(cfg, bank, ms)
     cu = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)
-    for _ in range(64):  # the benchmark's pre-roll: the pool reaches the steady state
+    # Pre-roll until the pool is saturated and stealing (about 65 blocks, the
+    # benchmark's pre-roll), then one more block of steady state.
+    steady = 0
+    for _ in range(120):
         H.feed(cu, drv.prepare(cu.stats().active_voices))
         cu.render()
         drv.finish(cu.stats().active_voices)
+        steady += cu.stats().stolen > 0
+        if steady == 2:
+            break
     st0 = cu.stats()
     assert st0.active_voices == cfg.max_voices and st0.stolen > 0
     orc = OracleSynth(cfg, bank.pool, bank.params, threads=os.cpu_count() or 1)
