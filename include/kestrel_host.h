@@ -185,6 +185,44 @@ float kh_timecents_to_secs(float tc);
  * Returns the output length. */
 size_t kh_resample_i16(const int16_t* src, size_t n, double ratio, int16_t* out, size_t cap);
 
+/* ---- the output stage ------------------------------------------------------
+ * What Driver::next_block does to the backend's block after render
+ * (src/driver.rs:596-606): the configured limiter, then clamp_block. Host
+ * side, on the mixed stereo block; state carries across blocks. */
+#define KH_LIMITER_OFF 0u
+#define KH_LIMITER_OMNI 1u       /* the OmniConverter loudness follower (src/limiter.rs:13-116) */
+#define KH_LIMITER_BRICKWALL 2u  /* lookahead true-peak brickwall (src/limiter.rs:164-441), the default */
+
+typedef struct kh_limiter kh_limiter;
+/* Config defaults: mode brickwall, ceiling 0 dB, lookahead 2 ms, release
+ * 60 ms, sustain 0 ms, true peak on (src/config.rs:387-393); ranges as
+ * Config::validate (src/config.rs:472-494). */
+kh_limiter* kh_limiter_create(uint32_t mode, uint32_t sample_rate, double ceiling_db, double lookahead_ms,
+                              double release_ms, double sustain_ms, int true_peak);
+void kh_limiter_destroy(kh_limiter* l);
+/* Frames the brickwall delays the render by (lookahead + detector delay). */
+uint32_t kh_limiter_latency(const kh_limiter* l);
+/* The limiter, then clamp_block, in place on n interleaved samples. Returns
+ * how many samples clamp_block had to move (Stats::clipped). */
+uint64_t kh_limiter_process(kh_limiter* l, float* buf, size_t n);
+/* Brickwall only: the largest detected input peak and the smallest gain. */
+int kh_limiter_report(const kh_limiter* l, double* peak_in, double* min_gain);
+/* clamp_block (src/limiter.rs:120-129): clamp to [-1, 1]; returns the count moved. */
+uint64_t kh_clamp_block(float* buf, size_t n);
+
+/* ---- WAV output (src/wav.rs:50-159) ---------------------------------------- */
+#define KH_WAV_PCM16 0u
+#define KH_WAV_FLOAT32 1u
+typedef struct kh_wav kh_wav;
+/* A RIFF/WAVE file with a 44-byte header whose sizes are patched at finish
+ * (saturated at 4 GiB, as the reference does). */
+kh_wav* kh_wav_create(const char* path, uint32_t sample_rate, uint16_t channels, uint32_t format);
+/* Append n interleaved samples: f32 as is, or pcm16 as
+ * round(clamp(s, -1, 1) * 32767). */
+int kh_wav_write(kh_wav* w, const float* samples, size_t n);
+/* Patch the header, close the file and free the writer. */
+int kh_wav_finish(kh_wav* w, uint64_t* data_bytes);
+
 /* A batch resampler the bank builder hands every sample it converts at load
  * (build_pool, src/sf2.rs:585-703) instead of running the host loop, e.g.
  * kc_resample_i16_batch on a GPU. Source i (src_len[i] frames) at ratio[i]

@@ -46,6 +46,9 @@ inline uint64_t rank_key(float gl, float gr, size_t index) {
 inline double rfract(double x) { return x - std::trunc(x); }
 }  // namespace
 
+std::string& last_error() { return g_err; }
+
+
 struct Driver {
     kc_config cfg{};
     kh_options opt{};

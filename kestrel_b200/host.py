@@ -86,6 +86,15 @@ HOST_SYMBOLS = {
     "kh_timecents_to_secs": (C.c_float, [C.c_float]),
     "kh_resample_i16": (C.c_size_t, [_P, C.c_size_t, C.c_double, _P, C.c_size_t]),
     "kh_set_resampler": (None, [_P, _P]),
+    "kh_limiter_create": (_P, [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]),
+    "kh_limiter_destroy": (None, [_P]),
+    "kh_limiter_latency": (C.c_uint32, [_P]),
+    "kh_limiter_process": (C.c_uint64, [_P, _P, C.c_size_t]),
+    "kh_limiter_report": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "kh_clamp_block": (C.c_uint64, [_P, C.c_size_t]),
+    "kh_wav_create": (_P, [C.c_char_p, C.c_uint32, C.c_uint16, C.c_uint32]),
+    "kh_wav_write": (C.c_int, [_P, _P, C.c_size_t]),
+    "kh_wav_finish": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "kh_sinc_table": (C.c_int, [C.c_double, _P, C.c_size_t]),
     "kh_mix48": (C.c_uint64, [C.c_uint64]),
     "kh_rank_gain_q": (C.c_uint64, [C.c_float, C.c_float]),
@@ -167,6 +176,73 @@ def resample_i16(src: np.ndarray, ratio: float) -> np.ndarray:
     out = np.empty(cap, np.int16)
     n = lib().kh_resample_i16(N.ptr(src), src.size, ratio, N.ptr(out), cap)
     return out[:n].copy()
+
+
+LIMITER_OFF, LIMITER_OMNI, LIMITER_BRICKWALL = 0, 1, 2
+WAV_PCM16, WAV_FLOAT32 = 0, 1
+
+
+class Limiter:
+    """The output stage after each render (src/driver.rs:596-606): the
+    limiter, then clamp_block. Defaults are the reference's config."""
+
+    def __init__(self, mode: int = LIMITER_BRICKWALL, sample_rate: int = 48000, ceiling_db: float = 0.0,
+                 lookahead_ms: float = 2.0, release_ms: float = 60.0, sustain_ms: float = 0.0,
+                 true_peak: bool = True):
+        self._lib = lib()
+        h = self._lib.kh_limiter_create(mode, sample_rate, ceiling_db, lookahead_ms, release_ms, sustain_ms,
+                                        1 if true_peak else 0)
+        if not h:
+            raise ValueError(self._lib.kh_last_error().decode())
+        self._h = h
+        self.clipped = 0
+
+    @property
+    def latency(self) -> int:
+        return self._lib.kh_limiter_latency(self._h)
+
+    def process(self, buf: np.ndarray) -> np.ndarray:
+        """In place on an interleaved f32 block; returns it."""
+        assert buf.dtype == np.float32 and buf.flags["C_CONTIGUOUS"]
+        self.clipped += self._lib.kh_limiter_process(self._h, N.ptr(buf), buf.size)
+        return buf
+
+    def report(self):
+        p, g = C.c_double(), C.c_double()
+        self._lib.kh_limiter_report(self._h, C.byref(p), C.byref(g))
+        return p.value, g.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.kh_limiter_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class WavWriter:
+    """WavWriter (src/wav.rs:50-159): pcm16 or float32, sizes patched at finish."""
+
+    def __init__(self, path, sample_rate: int = 48000, channels: int = 2, fmt: int = WAV_FLOAT32):
+        self._lib = lib()
+        h = self._lib.kh_wav_create(str(path).encode(), sample_rate, channels, fmt)
+        if not h:
+            raise OSError(self._lib.kh_last_error().decode())
+        self._h = h
+
+    def write(self, block: np.ndarray) -> None:
+        block = np.ascontiguousarray(block, dtype=np.float32)
+        if self._lib.kh_wav_write(self._h, N.ptr(block), block.size) != 0:
+            raise OSError("wav write failed")
+
+    def finish(self) -> int:
+        n = C.c_uint64()
+        rc = self._lib.kh_wav_finish(self._h, C.byref(n))
+        self._h = None
+        if rc != 0:
+            raise OSError("wav finish failed")
+        return n.value
 
 
 def sinc_table(ratio: float) -> np.ndarray:
