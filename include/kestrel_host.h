@@ -119,6 +119,35 @@ typedef struct kh_midi_spec {
 
 void kh_midi_spec_default(kh_midi_spec* s);
 
+/* ---- standard MIDI files (src/midi.rs) ------------------------------------ */
+
+/* A standard MIDI file read as one tick-ordered event stream: every track
+ * read through its own 256 KiB window and merged by (tick, track index)
+ * (MidiStream, src/midi.rs:239-374). For tests and tools; the driver opens
+ * files itself (kh_driver_open_smf). */
+typedef struct kh_smf kh_smf;
+#define KH_EV_NOTE_ON 0u
+#define KH_EV_NOTE_OFF 1u
+#define KH_EV_CC 2u
+#define KH_EV_PROGRAM 3u
+#define KH_EV_PITCH_BEND 4u
+#define KH_EV_TEMPO 5u
+#define KH_EV_OTHER 6u
+kh_smf* kh_smf_open(const char* path);
+void kh_smf_close(kh_smf* m);
+/* format, track count; ppq, or 0 with the SMPTE frames per second and ticks
+ * per frame. */
+int kh_smf_info(const kh_smf* m, uint16_t* format, uint16_t* tracks, uint32_t* ppq, uint8_t* fps,
+                uint8_t* ticks_per_frame);
+/* The next event: 1, or 0 at the end. a/b are key/velocity (notes), number/
+ * value (CC), program; bend is -8192..8191; tempo in microseconds per quarter. */
+int kh_smf_next(kh_smf* m, uint64_t* tick, uint32_t* type, uint8_t* ch, uint8_t* a, uint8_t* b, int16_t* bend,
+                uint32_t* tempo);
+/* Write the synthetic stream of `spec` (up to max_events events, 0: all) as
+ * a format-1 SMF of one track at the spec's ppq, full status bytes, the way
+ * MidiWriter does (src/midi.rs:439-506). */
+int kh_midi_write_synthetic(const kh_midi_spec* spec, const char* path, uint64_t max_events);
+
 /* ---- the driver ---------------------------------------------------------- */
 
 typedef struct kh_driver kh_driver;
@@ -143,6 +172,9 @@ typedef struct kh_block {
 
 kh_driver* kh_driver_open(const kc_config* cfg, const kh_options* opt, const kh_bank* bank,
                           const kh_midi_spec* midi);
+/* The same driver reading a standard MIDI file (Driver::open,
+ * src/driver.rs:343-413). Null with kh_last_error() set if it cannot be read. */
+kh_driver* kh_driver_open_smf(const kc_config* cfg, const kh_options* opt, const kh_bank* bank, const char* path);
 void kh_driver_destroy(kh_driver* d);
 
 /* Driver::next_block (src/driver.rs:434-594) up to the backend's spawn:

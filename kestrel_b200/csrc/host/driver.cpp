@@ -54,7 +54,7 @@ struct Driver {
     kh_options opt{};
     BankConfig bcfg;
     const Bank* bank = nullptr;
-    std::unique_ptr<SynthMidi> stream;
+    std::unique_ptr<EventSource> stream;
     TempoClock clock;
     GateTable gates;
     ChannelTable chan;
@@ -99,15 +99,19 @@ struct Driver {
     uint32_t last_want = 0, last_take = 0, last_live = 0;
 
     // Driver::open, src/driver.rs:343-413.
-    Driver(const kc_config& c, const kh_options& o, const Bank& b, const kh_midi_spec& m) : cfg(c), opt(o), bank(&b) {
+    // The event source is the synthetic stream of `m`, or `file` when given.
+    Driver(const kc_config& c, const kh_options& o, const Bank& b, const kh_midi_spec& m,
+           std::unique_ptr<EventSource> file = nullptr)
+        : cfg(c), opt(o), bank(&b) {
         bcfg.sample_rate = c.sample_rate;
         bcfg.env_floor = c.env_floor;
         bcfg.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
         bcfg.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
         bcfg.filter_enabled = o.filter_enabled != 0;
         bcfg.master_volume = o.master_volume;
-        stream = std::make_unique<SynthMidi>(m);
-        clock = TempoClock(stream->ppq(), c.sample_rate);
+        if (file) stream = std::move(file);
+        else stream = std::make_unique<SynthMidi>(m);
+        clock = TempoClock(stream->division(), c.sample_rate);
         gates.init(c.block_frames, c.gate_frames);
         chan.init(c.block_frames, c.gate_frames);
         for (int i = 0; i < 16; ++i) {
@@ -755,6 +759,31 @@ kh_driver* kh_driver_open(const kc_config* cfg, const kh_options* opt, const kh_
     return d;
 }
 
+kh_driver* kh_driver_open_smf(const kc_config* cfg, const kh_options* opt, const kh_bank* bank, const char* path) {
+    if (!cfg || !bank || !path) {
+        g_err = "null argument";
+        return nullptr;
+    }
+    if (cfg->gate_frames == 0 || cfg->block_frames % cfg->gate_frames) {
+        g_err = "gate_frames must divide block_frames";
+        return nullptr;
+    }
+    std::string err;
+    std::unique_ptr<SmfStream> file = SmfStream::open(path, &err);
+    if (!file) {
+        g_err = err;
+        return nullptr;
+    }
+    kh_options o;
+    kh_options_default(&o);
+    if (opt) o = *opt;
+    kh_midi_spec unused;
+    kh_midi_spec_default(&unused);
+    auto* d = new kh_driver();
+    d->d = std::make_unique<Driver>(*cfg, o, bank->bank, unused, std::move(file));
+    return d;
+}
+
 void kh_driver_destroy(kh_driver* d) { delete d; }
 
 int kh_driver_prepare(kh_driver* h, uint32_t live, kh_block* out) {
@@ -843,5 +872,128 @@ int kh_sinc_table(double ratio, float* out, size_t cap) {
 }
 uint64_t kh_mix48(uint64_t index) { return mix48(index); }
 uint64_t kh_rank_gain_q(float gain_l, float gain_r) { return rank_gain_q(gain_l, gain_r); }
+
+}  // extern "C"
+
+// ---- standard MIDI files ------------------------------------------------------
+
+struct kh_smf {
+    std::unique_ptr<kh::SmfStream> s;
+};
+
+namespace {
+void write_varlen(std::vector<uint8_t>& buf, uint64_t v) {
+    uint8_t stack[10];
+    int n = 0;
+    stack[n++] = (uint8_t)(v & 0x7F);
+    v >>= 7;
+    while (v > 0) {
+        stack[n++] = (uint8_t)((v & 0x7F) | 0x80);
+        v >>= 7;
+    }
+    for (int i = n - 1; i >= 0; --i) buf.push_back(stack[i]);
+}
+void put_be32(std::vector<uint8_t>& b, uint32_t v) {
+    for (int s = 24; s >= 0; s -= 8) b.push_back((uint8_t)(v >> s));
+}
+}  // namespace
+
+extern "C" {
+
+kh_smf* kh_smf_open(const char* path) {
+    if (!path) {
+        g_err = "null path";
+        return nullptr;
+    }
+    std::string err;
+    auto s = kh::SmfStream::open(path, &err);
+    if (!s) {
+        g_err = err;
+        return nullptr;
+    }
+    auto* m = new kh_smf();
+    m->s = std::move(s);
+    return m;
+}
+
+void kh_smf_close(kh_smf* m) { delete m; }
+
+int kh_smf_info(const kh_smf* m, uint16_t* format, uint16_t* tracks, uint32_t* ppq, uint8_t* fps,
+                uint8_t* ticks_per_frame) {
+    if (!m) return 1;
+    const kh::Division d = m->s->division();
+    if (format) *format = m->s->format();
+    if (tracks) *tracks = m->s->tracks();
+    if (ppq) *ppq = d.smpte ? 0 : d.ppq;
+    if (fps) *fps = d.fps;
+    if (ticks_per_frame) *ticks_per_frame = d.ticks_per_frame;
+    return 0;
+}
+
+int kh_smf_next(kh_smf* m, uint64_t* tick, uint32_t* type, uint8_t* ch, uint8_t* a, uint8_t* b, int16_t* bend,
+                uint32_t* tempo) {
+    kh::Event ev;
+    uint64_t t = 0;
+    if (!m || !m->s->next(&t, &ev)) return 0;
+    if (tick) *tick = t;
+    if (type) *type = (uint32_t)ev.type;
+    if (ch) *ch = ev.ch;
+    if (a) *a = ev.a;
+    if (b) *b = ev.b;
+    if (bend) *bend = ev.bend;
+    if (tempo) *tempo = ev.tempo;
+    return 1;
+}
+
+int kh_midi_write_synthetic(const kh_midi_spec* spec, const char* path, uint64_t max_events) {
+    if (!spec || !path) {
+        g_err = "null argument";
+        return 1;
+    }
+    kh::SynthMidi src(*spec);
+    std::vector<uint8_t> trk;
+    uint64_t last = 0, t = 0, n = 0;
+    kh::Event ev;
+    while ((max_events == 0 || n < max_events) && src.next(&t, &ev)) {
+        write_varlen(trk, t - last);
+        last = t;
+        const uint8_t c = ev.ch & 0x0F;
+        switch (ev.type) {
+            case kh::EvType::NoteOn: trk.insert(trk.end(), {(uint8_t)(0x90 | c), ev.a, ev.b}); break;
+            case kh::EvType::NoteOff: trk.insert(trk.end(), {(uint8_t)(0x80 | c), ev.a, 0}); break;
+            case kh::EvType::Cc: trk.insert(trk.end(), {(uint8_t)(0xB0 | c), ev.a, ev.b}); break;
+            case kh::EvType::Program: trk.insert(trk.end(), {(uint8_t)(0xC0 | c), ev.a}); break;
+            case kh::EvType::PitchBend: {
+                const uint16_t raw = (uint16_t)(ev.bend + 8192);
+                trk.insert(trk.end(), {(uint8_t)(0xE0 | c), (uint8_t)(raw & 0x7F), (uint8_t)((raw >> 7) & 0x7F)});
+                break;
+            }
+            case kh::EvType::Tempo:
+                trk.insert(trk.end(), {0xFF, 0x51, 0x03, (uint8_t)(ev.tempo >> 16), (uint8_t)(ev.tempo >> 8),
+                                       (uint8_t)ev.tempo});
+                break;
+            default:
+                trk.insert(trk.end(), {0xFF, 0x01, 0x00});  // an empty text event
+                break;
+        }
+        ++n;
+    }
+    write_varlen(trk, 0);
+    trk.insert(trk.end(), {0xFF, 0x2F, 0x00});
+    std::vector<uint8_t> out = {'M', 'T', 'h', 'd', 0, 0, 0, 6, 0, 1, 0, 1};
+    const uint16_t ppq = (uint16_t)std::min<uint32_t>(spec->ppq ? spec->ppq : 9600, 0x7FFF);
+    out.push_back((uint8_t)(ppq >> 8));
+    out.push_back((uint8_t)ppq);
+    out.insert(out.end(), {'M', 'T', 'r', 'k'});
+    put_be32(out, (uint32_t)trk.size());
+    out.insert(out.end(), trk.begin(), trk.end());
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        g_err = std::string("cannot create ") + path;
+        return 1;
+    }
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    return std::fclose(f) == 0 && ok ? 0 : 1;
+}
 
 }  // extern "C"

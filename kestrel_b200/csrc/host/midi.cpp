@@ -1,5 +1,10 @@
-// midi.cpp -- the seeded synthetic event stream.
+// midi.cpp -- the driver's event sources: the seeded synthetic stream and
+// standard MIDI files.
 #include "midi.h"
+
+#include <cstdio>
+#include <cstring>
+#include <functional>
 
 namespace kh {
 
@@ -216,6 +221,252 @@ bool SynthMidi::next(uint64_t* tick, Event* ev) {
     uint64_t off = tick_of((double)o.tick / ticks_per_s_ + o.dur_s);
     if (off <= o.tick) off = o.tick + 1;
     offs_.push(Off{off, off_seq_++, o.ch, o.key});  // (tick, seq) order, as pops return them
+    return true;
+}
+
+}  // namespace kh
+
+// ---- standard MIDI files ---------------------------------------------------------
+
+namespace kh {
+
+namespace {
+constexpr size_t TRACK_BUF = 256 * 1024;
+
+uint32_t be32(const uint8_t* p) { return (uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3]; }
+uint16_t be16(const uint8_t* p) { return (uint16_t)(p[0] << 8 | p[1]); }
+}  // namespace
+
+// TrackReader (src/midi.rs:39-236): one track chunk with its own file handle
+// and read window; decodes one event at a time, keeping running status.
+struct SmfStream::Track {
+    std::FILE* f = nullptr;
+    std::vector<uint8_t> buf;
+    size_t pos = 0, filled = 0;
+    uint64_t remaining = 0;
+    uint64_t tick = 0;
+    uint8_t running = 0;
+    bool ended = false;
+
+    ~Track() {
+        if (f) std::fclose(f);
+    }
+    bool fill() {
+        if (remaining == 0) return false;
+        const size_t want = (size_t)std::min<uint64_t>(remaining, TRACK_BUF);
+        const size_t got = std::fread(buf.data(), 1, want, f);
+        remaining -= got;
+        pos = 0;
+        filled = got;
+        return got > 0;
+    }
+    bool byte(uint8_t* b) {
+        if (pos == filled && !fill()) return false;
+        *b = buf[pos++];
+        return true;
+    }
+    bool varlen(uint64_t* v) {
+        *v = 0;
+        for (int i = 0; i < 8; ++i) {
+            uint8_t b;
+            if (!byte(&b)) return false;
+            *v = (*v << 7) | (uint64_t)(b & 0x7F);
+            if (!(b & 0x80)) return true;
+        }
+        return false;
+    }
+    bool skip(uint64_t n) {
+        while (n > 0) {
+            if (pos == filled && !fill()) return false;
+            const uint64_t take = std::min<uint64_t>(filled - pos, n);
+            pos += (size_t)take;
+            n -= take;
+        }
+        return true;
+    }
+    // TrackReader::next_event (src/midi.rs:126-236). False at the end of the
+    // track, or where it stops making sense.
+    bool next_event(Event* ev) {
+        if (ended) return false;
+        auto end = [&] {
+            ended = true;
+            return false;
+        };
+        uint64_t delta;
+        if (!varlen(&delta)) return end();
+        tick += delta;
+        uint8_t status;
+        if (!byte(&status)) return end();
+        uint8_t first = 0;
+        if (status < 0x80) {
+            // Running status: the byte is the first data byte of a message
+            // with the previous channel status.
+            first = status;
+            status = running;
+            if (status < 0x80) return end();  // data before any status byte
+        } else {
+            if (status < 0xF0) running = status;
+            else if (status == 0xFF) running = 0;  // only meta clears it
+            if (status != 0xFF && status != 0xF0 && status != 0xF7 && !byte(&first)) return end();
+        }
+        const uint8_t ch = status & 0x0F;
+        *ev = Event{};
+        ev->ch = ch;
+        uint8_t b2;
+        switch (status & 0xF0) {
+            case 0x80:
+                if (!byte(&b2)) return false;
+                ev->type = EvType::NoteOff;
+                ev->a = first & 0x7F;
+                return true;
+            case 0x90:
+                if (!byte(&b2)) return false;
+                ev->a = first & 0x7F;
+                if (b2 == 0) {
+                    ev->type = EvType::NoteOff;
+                } else {
+                    ev->type = EvType::NoteOn;
+                    ev->b = b2 & 0x7F;
+                }
+                return true;
+            case 0xA0:
+                if (!byte(&b2)) return false;
+                ev->type = EvType::Other;
+                return true;
+            case 0xB0:
+                if (!byte(&b2)) return false;
+                ev->type = EvType::Cc;
+                ev->a = first & 0x7F;
+                ev->b = b2 & 0x7F;
+                return true;
+            case 0xC0:
+                ev->type = EvType::Program;
+                ev->a = first & 0x7F;
+                return true;
+            case 0xD0:
+                ev->type = EvType::Other;
+                return true;
+            case 0xE0: {
+                if (!byte(&b2)) return false;
+                const int16_t raw = (int16_t)(((int16_t)(b2 & 0x7F) << 7) | (int16_t)(first & 0x7F));
+                ev->type = EvType::PitchBend;
+                ev->bend = (int16_t)(raw - 8192);
+                return true;
+            }
+            default:
+                break;
+        }
+        ev->type = EvType::Other;
+        ev->ch = 0;
+        if (status == 0xFF) {
+            uint8_t meta;
+            uint64_t len;
+            if (!byte(&meta) || !varlen(&len)) return false;
+            if (meta == 0x2F) {
+                if (!skip(len)) return false;
+                ended = true;
+                return true;
+            }
+            if (meta == 0x51 && len == 3) {
+                uint8_t a, b, c;
+                if (!byte(&a) || !byte(&b) || !byte(&c)) return false;
+                ev->type = EvType::Tempo;
+                ev->tempo = (uint32_t)a << 16 | (uint32_t)b << 8 | c;
+                return true;
+            }
+            return skip(len);
+        }
+        if (status == 0xF0 || status == 0xF7) {
+            uint64_t len;
+            if (!varlen(&len)) return false;
+            return skip(len);
+        }
+        return true;  // other system messages carry no data here
+    }
+};
+
+SmfStream::~SmfStream() = default;
+
+// MidiStream::open (src/midi.rs:259-363).
+std::unique_ptr<SmfStream> SmfStream::open(const std::string& path, std::string* err) {
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) {
+        *err = "opening " + path;
+        return nullptr;
+    }
+    std::fseek(f, 0, SEEK_END);
+    const uint64_t file_len = (uint64_t)std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    uint8_t hdr[14];
+    if (std::fread(hdr, 1, 14, f) != 14) {
+        std::fclose(f);
+        *err = path + ": too short for an SMF header";
+        return nullptr;
+    }
+    if (std::memcmp(hdr, "MThd", 4) != 0) {
+        std::fclose(f);
+        *err = path + ": not a standard MIDI file";
+        return nullptr;
+    }
+    std::unique_ptr<SmfStream> s(new SmfStream());
+    const uint64_t hdr_len = be32(hdr + 4);
+    s->format_ = be16(hdr + 8);
+    const int16_t div_raw = (int16_t)be16(hdr + 12);
+    if (div_raw > 0) {
+        s->division_.ppq = (uint32_t)div_raw;
+    } else {
+        s->division_.smpte = true;
+        s->division_.fps = (uint8_t)(-(div_raw >> 8));
+        s->division_.ticks_per_frame = (uint8_t)(div_raw & 0xFF);
+    }
+    // Walk the chunk headers; a zero-length unknown chunk is trailing padding
+    // (exporters pad with zeros), where the walk stops.
+    std::vector<std::pair<uint64_t, uint64_t>> locs;
+    uint64_t offset = 8 + hdr_len;
+    while (offset + 8 <= file_len) {
+        uint8_t ch[8];
+        if (std::fseek(f, (long)offset, SEEK_SET) != 0 || std::fread(ch, 1, 8, f) != 8) break;
+        const uint64_t data_start = offset + 8;
+        const uint64_t len = std::min<uint64_t>(be32(ch + 4), file_len > data_start ? file_len - data_start : 0);
+        if (std::memcmp(ch, "MTrk", 4) == 0) locs.emplace_back(data_start, len);
+        else if (len == 0) break;
+        offset = data_start + len;
+    }
+    std::fclose(f);
+    if (locs.empty()) {
+        *err = path + ": no MTrk chunks";
+        return nullptr;
+    }
+    for (const auto& [off, len] : locs) {
+        auto t = std::make_unique<Track>();
+        t->f = std::fopen(path.c_str(), "rb");
+        if (!t->f || std::fseek(t->f, (long)off, SEEK_SET) != 0) {
+            *err = "opening " + path;
+            return nullptr;
+        }
+        t->buf.resize(TRACK_BUF);
+        t->remaining = len;
+        s->readers_.push_back(std::move(t));
+    }
+    s->pending_.resize(s->readers_.size());
+    for (uint32_t i = 0; i < s->readers_.size(); ++i)
+        if (s->readers_[i]->next_event(&s->pending_[i])) s->heap_.emplace_back(s->readers_[i]->tick, i);
+    std::make_heap(s->heap_.begin(), s->heap_.end(), std::greater<>());
+    return s;
+}
+
+// MidiStream::next (src/midi.rs:365-374): the smallest (tick, track) first.
+bool SmfStream::next(uint64_t* tick, Event* ev) {
+    if (heap_.empty()) return false;
+    std::pop_heap(heap_.begin(), heap_.end(), std::greater<>());
+    const auto [t, i] = heap_.back();
+    heap_.pop_back();
+    *tick = t;
+    *ev = pending_[i];
+    if (readers_[i]->next_event(&pending_[i])) {
+        heap_.emplace_back(readers_[i]->tick, i);
+        std::push_heap(heap_.begin(), heap_.end(), std::greater<>());
+    }
     return true;
 }
 

@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstdint>
 #include <deque>
+#include <memory>
+#include <string>
 #include <random>
 #include <vector>
 
@@ -23,26 +25,73 @@ struct Event {
     uint32_t tempo = 0;            // microseconds per quarter note
 };
 
-// TempoClock (src/midi.rs:378-431), PPQ division only.
-struct TempoClock {
-    double sample_rate = 48000.0;
+// midi::Division (src/midi.rs:31-37).
+struct Division {
+    bool smpte = false;
     uint32_t ppq = 960;
+    uint8_t fps = 0, ticks_per_frame = 0;
+};
+
+// TempoClock (src/midi.rs:378-431): ticks to output frames, following tempo
+// changes as they arrive in the merged stream. SMPTE division ignores tempo.
+struct TempoClock {
+    Division division;
+    double sample_rate = 48000.0;
     uint64_t base_tick = 0;
     double base_frame = 0.0;
     double frames_per_tick = 0.0;
 
     TempoClock() = default;
-    TempoClock(uint32_t ppq_, uint32_t rate) : sample_rate((double)rate), ppq(ppq_) { set_tempo_raw(500000); }
+    TempoClock(Division d, uint32_t rate) : division(d), sample_rate((double)rate) { set_tempo_raw(500000); }
     void set_tempo_raw(uint32_t us_per_qn) {
-        const double p = (double)std::max<uint32_t>(ppq, 1);
-        frames_per_tick = ((double)us_per_qn * 1e-6) * sample_rate / p;
+        if (division.smpte) {
+            const double tps = (double)std::max<uint8_t>(division.fps, 1) *
+                               (double)std::max<uint8_t>(division.ticks_per_frame, 1);
+            frames_per_tick = sample_rate / tps;
+        } else {
+            const double p = (double)std::max<uint32_t>(division.ppq, 1);
+            frames_per_tick = ((double)us_per_qn * 1e-6) * sample_rate / p;
+        }
     }
     void set_tempo(uint64_t tick, uint32_t us_per_qn) {
+        if (division.smpte) return;
         base_frame = frame_at(tick);
         base_tick = tick;
         set_tempo_raw(us_per_qn);
     }
     double frame_at(uint64_t tick) const { return base_frame + (double)(tick - base_tick) * frames_per_tick; }
+};
+
+// Where the driver's events come from: a MIDI file or the synthetic stream.
+class EventSource {
+   public:
+    virtual ~EventSource() = default;
+    // Next event in tick order; false when the stream is exhausted.
+    virtual bool next(uint64_t* tick, Event* ev) = 0;
+    virtual Division division() const = 0;
+};
+
+// MidiStream (src/midi.rs:239-374): a standard MIDI file read a window at a
+// time per track (256 KiB each, so a 40 GB file costs the memory of a small
+// one) and merged into one tick-ordered stream, ties broken by track index.
+class SmfStream : public EventSource {
+   public:
+    // Returns null (with `err` set) when the file is not a usable SMF.
+    static std::unique_ptr<SmfStream> open(const std::string& path, std::string* err);
+    ~SmfStream() override;
+    bool next(uint64_t* tick, Event* ev) override;
+    Division division() const override { return division_; }
+    uint16_t format() const { return format_; }
+    uint16_t tracks() const { return (uint16_t)readers_.size(); }
+
+   private:
+    struct Track;
+    SmfStream() = default;
+    std::vector<std::unique_ptr<Track>> readers_;
+    std::vector<Event> pending_;
+    std::vector<std::pair<uint64_t, uint32_t>> heap_;  // min-heap of (tick, track)
+    Division division_;
+    uint16_t format_ = 0;
 };
 
 // Pending note-offs, popped in (tick, seq) order. A calendar queue: one
@@ -81,12 +130,16 @@ class OffQueue {
 // Controller curves and program changes run on their own schedule. The three
 // sources are merged by tick (at equal ticks: offs, then controllers, then
 // ons), so the stream is a pure function of the spec.
-class SynthMidi {
+class SynthMidi : public EventSource {
    public:
     explicit SynthMidi(const kh_midi_spec& s);
     // Next event in tick order; false when the stream is exhausted.
-    bool next(uint64_t* tick, Event* ev);
-    uint32_t ppq() const { return spec_.ppq; }
+    bool next(uint64_t* tick, Event* ev) override;
+    Division division() const override {
+        Division d;
+        d.ppq = spec_.ppq;
+        return d;
+    }
 
    private:
     using Off = OffQueue::Off;

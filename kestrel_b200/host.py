@@ -65,6 +65,15 @@ HOST_SYMBOLS = {
     "kh_midi_spec_default": (None, [C.POINTER(KhMidiSpec)]),
     "kh_driver_open": (_P, [C.POINTER(N.KcConfig), C.POINTER(KhOptions), _P, C.POINTER(KhMidiSpec)]),
     "kh_driver_destroy": (None, [_P]),
+    "kh_driver_open_smf": (_P, [C.POINTER(N.KcConfig), C.POINTER(KhOptions), _P, C.c_char_p]),
+    "kh_smf_open": (_P, [C.c_char_p]),
+    "kh_smf_close": (None, [_P]),
+    "kh_smf_info": (C.c_int, [_P, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.POINTER(C.c_uint32),
+                              C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
+    "kh_smf_next": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint8),
+                              C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(C.c_int16),
+                              C.POINTER(C.c_uint32)]),
+    "kh_midi_write_synthetic": (C.c_int, [C.POINTER(KhMidiSpec), C.c_char_p, C.c_uint64]),
     "kh_driver_prepare": (C.c_int, [_P, C.c_uint32, C.POINTER(KhBlock)]),
     "kh_driver_variant": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "kh_driver_finish": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
@@ -176,6 +185,40 @@ def resample_i16(src: np.ndarray, ratio: float) -> np.ndarray:
     out = np.empty(cap, np.int16)
     n = lib().kh_resample_i16(N.ptr(src), src.size, ratio, N.ptr(out), cap)
     return out[:n].copy()
+
+
+EV_NAMES = ["note_on", "note_off", "cc", "program", "pitch_bend", "tempo", "other"]
+
+
+def read_smf(path):
+    """(info, events) of a standard MIDI file: info = (format, tracks, ppq,
+    fps, ticks_per_frame), events = [(tick, kind, ch, a, b, bend, tempo)] in
+    merged tick order (MidiStream, src/midi.rs:239-374)."""
+    L = lib()
+    h = L.kh_smf_open(str(path).encode())
+    if not h:
+        raise RuntimeError(L.kh_last_error().decode())
+    try:
+        f, t, q = C.c_uint16(), C.c_uint16(), C.c_uint32()
+        fps, tpf = C.c_uint8(), C.c_uint8()
+        L.kh_smf_info(h, C.byref(f), C.byref(t), C.byref(q), C.byref(fps), C.byref(tpf))
+        info = (f.value, t.value, q.value, fps.value, tpf.value)
+        ev = []
+        tick, typ = C.c_uint64(), C.c_uint32()
+        ch, a, b = C.c_uint8(), C.c_uint8(), C.c_uint8()
+        bend, tempo = C.c_int16(), C.c_uint32()
+        while L.kh_smf_next(h, C.byref(tick), C.byref(typ), C.byref(ch), C.byref(a), C.byref(b), C.byref(bend),
+                            C.byref(tempo)):
+            ev.append((tick.value, EV_NAMES[typ.value], ch.value, a.value, b.value, bend.value, tempo.value))
+        return info, ev
+    finally:
+        L.kh_smf_close(h)
+
+
+def write_synthetic_midi(spec: KhMidiSpec, path, max_events: int = 0) -> None:
+    """The synthetic stream of `spec` as a format-1, one-track SMF."""
+    if lib().kh_midi_write_synthetic(C.byref(spec), str(path).encode(), max_events) != 0:
+        raise OSError(lib().kh_last_error().decode())
 
 
 LIMITER_OFF, LIMITER_OMNI, LIMITER_BRICKWALL = 0, 1, 2
@@ -358,10 +401,16 @@ class BlockInputs:
 
 
 class Driver:
-    def __init__(self, cfg: N.KcConfig, bank: Bank, midi: KhMidiSpec):
+    """Driver::next_block's host side over a synthetic MIDI spec, or over a
+    standard MIDI file when `midi` is a path."""
+
+    def __init__(self, cfg: N.KcConfig, bank: Bank, midi):
         self._lib = lib()
         self.bank = bank
-        h = self._lib.kh_driver_open(C.byref(cfg), C.byref(bank.opt), bank._h, C.byref(midi))
+        if isinstance(midi, KhMidiSpec):
+            h = self._lib.kh_driver_open(C.byref(cfg), C.byref(bank.opt), bank._h, C.byref(midi))
+        else:
+            h = self._lib.kh_driver_open_smf(C.byref(cfg), C.byref(bank.opt), bank._h, str(midi).encode())
         if not h:
             raise RuntimeError(self._lib.kh_last_error().decode())
         self._h = h

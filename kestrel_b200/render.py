@@ -1,6 +1,6 @@
 """Render a workload to a WAV file: the reference's render loop end to end.
 
-    python -m kestrel_b200.render --workload plain --out plain.wav
+    python -m kestrel_b200.render --workload plain --out plain.wav [--midi FILE.mid]
         [--limiter brickwall|omni|off] [--format float32|pcm16] [--seconds S]
 
 The loop of src/bin/kestrel.rs:311-365 around Driver::next_block
@@ -44,9 +44,9 @@ def cuda_backend(cfg, bank: H.Bank):
 def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: int = H.LIMITER_BRICKWALL,
                 fmt: int = H.WAV_FLOAT32, max_seconds: float = 0.0, limiter_opts: dict | None = None,
                 on_block=None) -> RenderStats:
-    """Render (cfg, soundfont spec, MIDI spec) into `path` until the stream
-    ends or `max_seconds` of audio (0: no bound). `backend(cfg, bank)` makes
-    the Backend (the CUDA one by default)."""
+    """Render (cfg, soundfont spec, MIDI spec or MIDI file path) into `path`
+    until the stream ends or `max_seconds` of audio (0: no bound).
+    `backend(cfg, bank)` makes the Backend (the CUDA one by default)."""
     bank = H.Bank(bank_spec, cfg)
     drv = H.Driver(cfg, bank, midi_spec)
     synth = backend(cfg, bank)
@@ -82,6 +82,7 @@ def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", choices=["plain", "black", "steal"], default="plain")
+    ap.add_argument("--midi", default=None, help="a standard MIDI file to render instead of the workload's stream")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--out", required=True)
     ap.add_argument("--limiter", choices=["brickwall", "omni", "off"], default="brickwall")
@@ -89,6 +90,8 @@ def main(argv=None) -> int:
     ap.add_argument("--seconds", type=float, default=0.0, help="stop after this much audio (0: the whole file)")
     args = ap.parse_args(argv)
     cfg, bs, ms = H.config_workload(args.workload, seed=args.seed)
+    if args.midi:
+        ms = args.midi
     mode = {"brickwall": H.LIMITER_BRICKWALL, "omni": H.LIMITER_OMNI, "off": H.LIMITER_OFF}[args.limiter]
     fmt = H.WAV_FLOAT32 if args.format == "float32" else H.WAV_PCM16
     st = render_file(args.out, cfg, bs, ms, limiter=mode, fmt=fmt, max_seconds=args.seconds)
