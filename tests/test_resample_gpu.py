@@ -18,8 +18,13 @@ from kestrel_b200 import native as N
 gpu = pytest.mark.gpu
 
 
+def _out_len(n, ratio):
+    """max(round(n * ratio), 1) with f64::round, which rounds halves away from zero."""
+    return max(int(np.floor(n * ratio + 0.5)), 1)
+
+
 def _host(src, ratio):
-    out = np.empty(int(max(round(src.size * ratio), 1)) + 1, np.int16)
+    out = np.empty(_out_len(src.size, ratio) + 1, np.int16)
     n = H.lib().kh_resample_i16(N.ptr(src), src.size, ratio, N.ptr(out), out.size)
     return out[:n].copy()
 
@@ -48,7 +53,7 @@ def test_device_batch_matches_host_loop():
         srcs.append(x.astype(np.int16))
         rs.append(ratios[i % len(ratios)])
     tabs = [H.sinc_table(r) for r in rs]
-    outs = [np.empty(int(max(round(s.size * r), 1)), np.int16) for s, r in zip(srcs, rs)]
+    outs = [np.empty(_out_len(s.size, r), np.int16) for s, r in zip(srcs, rs)]
     n = len(srcs)
     P = C.c_void_p * n
     src_p = P(*[s.ctypes.data for s in srcs])
