@@ -318,12 +318,13 @@ __device__ __forceinline__ bool env_transition(VoiceRegs& v, const RenderArgs& a
 
 // Can this lane run the tile starting at f0 on the fast path? Idle lanes
 // (no voice, dead, or starting after the tile) qualify trivially.
-// NF is the span checked: one 16-frame tile, or the two tiles of a 32-frame
-// gate tile.
+// NF is the span checked: one 16-frame tile, the two tiles of a 32-frame
+// gate tile, or the eight tiles of 128 frames.
 template <uint32_t NF>
 __device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a, uint32_t f0, bool looping,
                                         bool& active) {
-    constexpr uint32_t LOG2 = NF == 32 ? 5 : 4;
+    static_assert(NF == 16 || NF == 32 || NF == 128, "span");
+    constexpr uint32_t LOG2 = NF == 128 ? 7 : (NF == 32 ? 5 : 4);
     active = v.neutral;  // runs every path, contributing +0
     if (v.neutral) return true;
     if (v.stage == ENV_DEAD || v.start_rel >= f0 + NF) return true;
@@ -393,13 +394,20 @@ __device__ __forceinline__ float fast_frame(VoiceRegs& v, const RenderArgs& a, E
 // non-negative one, from a non-negative level), so the last frame's level
 // bounds every frame's. When it holds, the frame is branch-free and the
 // compiler can overlap consecutive frames (and the lane's voices).
+//
+// The margin covers, relative to the level: NF sequential roundings of half an
+// ulp (NF * 2^-24), the rounding of em^NF by squaring (each squaring doubles
+// the relative error and adds one rounding: up to (NF - 1) * 2^-24) and that
+// of the test itself. 1e-5 (168 * 2^-24) covers NF <= 32 with room; 128-frame
+// spans need (2 * 128 + 2) * 2^-24 = 1.5e-5 and take 4e-5.
 template <uint32_t NF>
 __device__ __forceinline__ bool no_transition(const VoiceRegs& v, const EnvStep& e) {
     constexpr float N = (float)NF;
+    constexpr float MARGIN = NF > 32 ? 4.0e-5f : 1.0e-5f;
     if (v.stage == ENV_SUSTAIN) return true;
     if (v.stage == ENV_ATTACK) {
         // level grows by attack_rate per frame towards attack_end
-        return e.ea >= 0.0f && v.level + N * e.ea + 1.0e-5f * fabsf(e.thr) < e.thr;
+        return e.ea >= 0.0f && v.level + N * e.ea + MARGIN * fabsf(e.thr) < e.thr;
     }
     const float thr = -e.thr;  // decay target or floor
     if (!(v.level >= 0.0f)) return false;
@@ -409,10 +417,14 @@ __device__ __forceinline__ bool no_transition(const VoiceRegs& v, const EnvStep&
         m *= m;
         m *= m;
         m *= m;
-        if (NF == 32) m *= m;
-        return v.level * m * (1.0f - 1.0e-5f) > thr;
+        if (NF >= 32) m *= m;
+        if (NF >= 128) {
+            m *= m;
+            m *= m;
+        }
+        return v.level * m * (1.0f - MARGIN) > thr;
     }
-    return e.ea <= 0.0f && v.level + N * e.ea - 1.0e-5f * v.level > thr;  // linear: ea = -coef
+    return e.ea <= 0.0f && v.level + N * e.ea - MARGIN * v.level > thr;  // linear: ea = -coef
 }
 
 // Under no_transition, is min(level, 1) == level on every frame of the tile?
@@ -731,19 +743,29 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
         }
         const bool first = b == gw;
 
-        // A tile's path comes from classifying it alone, or -- at the start
-        // of a 32-frame gate tile -- both of its tiles at once: when the
-        // whole span is hot, the second tile reuses the result (and the
-        // envelope constants, which no hot frame changes).
+        // A tile's path comes from classifying it alone, or from classifying
+        // a longer span at once -- 128 frames, else the 32-frame gate tile --
+        // whose later tiles then reuse the result (and the envelope
+        // constants, which no hot frame changes). A gate row met inside a
+        // carried span that changes any lane's stage (a release), step (a
+        // bend) or params variant ends the carry.
         EnvStep e[V];
         bool looping[V], active[V];
         int carried = -1, fm = FM_LANE;
+        uint32_t carry_left = 0;  // tiles of the current span still to run on `carried`
         uint32_t next_gate = 0, gt = 0;
         const bool span32 = a.gate_frames % 32u == 0u;
         for (uint32_t f0 = 0; f0 < a.block_frames; f0 += MIX_TILE) {
             if (f0 == next_gate) {
+                bool changed = false;
 #pragma unroll
-                for (int k = 0; k < V; ++k) tile_update<CHAN>(v[k], a, gt, chan_active);
+                for (int k = 0; k < V; ++k) {
+                    const uint32_t st = v[k].stage, var = v[k].variant;
+                    const uint64_t sp = v[k].step;
+                    tile_update<CHAN>(v[k], a, gt, chan_active);
+                    changed = changed || st != v[k].stage || sp != v[k].step || var != v[k].variant;
+                }
+                if (carry_left && __any_sync(0xFFFFFFFFu, changed)) carry_left = 0;
                 ++gt;
                 next_gate += a.gate_frames;
             }
@@ -753,9 +775,9 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
             float part_prev = 0.0f;
             if (MIX == KC_MIX_F32_TREE && !first) part_prev = part[j];
             int path;
-            if (carried >= 0) {
+            if (carry_left) {
                 path = carried;
-                carried = -1;
+                --carry_left;
             } else {
                 if (F32) {
 #pragma unroll
@@ -763,11 +785,16 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                         if (v[k].stage == ENV_DEAD && !v[k].neutral) neutralize(v[k], a);
                 }
                 path = P_GENERAL;
-                if (span32 && (f0 & 31u) == 0u) {
-                    path = classify<INTERP, V, 32>(v, a, f0, looping, active, e, fm);
-                    if (path <= P_HOT) carried = path;
+                if (span32 && (f0 & 127u) == 0u && f0 + 128u <= a.block_frames) {
+                    path = classify<INTERP, V, 128>(v, a, f0, looping, active, e, fm);
+                    if (path <= P_HOT) carry_left = 128u / MIX_TILE - 1u;
                 }
-                if (carried < 0) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e, fm);
+                if (!carry_left && span32 && (f0 & 31u) == 0u) {
+                    path = classify<INTERP, V, 32>(v, a, f0, looping, active, e, fm);
+                    if (path <= P_HOT) carry_left = 32u / MIX_TILE - 1u;
+                }
+                if (!carry_left) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e, fm);
+                carried = path;
             }
             if (path <= P_HOT) {
                 if (fm == FM_ALL) hot_dispatch<INTERP, FM_ALL, STRICT, F32, V>(path, v, a, e, sm, lane);

@@ -87,11 +87,13 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
                   admit_rule=N.ADMIT_LOUDEST, interpolation=N.INTERP_LINEAR, sort_voices: int = 0,
                   mix_mode=N.MIX_F32_TREE, strict_fp: int = 1, steal_percent: int = 25,
                   release_rate: float = 0.3, steps: str = "ratio", decay_curve=N.CURVE_EXPONENTIAL,
-                  release_curve=N.CURVE_EXPONENTIAL, voices_per_lane: int = 0, sort_radix_bits: int = 0) -> Scenario:
+                  release_curve=N.CURVE_EXPONENTIAL, voices_per_lane: int = 0, sort_radix_bits: int = 0,
+                  bend_prob: float = 1.0) -> Scenario:
     """steps: "ratio" (pitch ratios 2^U(-1.5, 1.5), random phase fractions),
     "unit" (every step exactly 1.0 and every phase fraction zero: the root key
     at the pool rate) or "integral" (steps of exactly 1, 2 or 3 with zero
-    phase fractions)."""
+    phase fractions). bend_prob < 1 leaves a channel's bend at exactly unity
+    on the other tiles (steps keep their whole-number ratio there)."""
     rng = np.random.default_rng(seed)
     cfg = N.default_config(max_voices=max_voices, block_frames=block_frames, gate_frames=gate_frames,
                            steal_rule=steal_rule, admit_rule=admit_rule, interpolation=interpolation,
@@ -163,6 +165,7 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
             off_count[rel] += 1
         chan_rows = np.zeros((tiles, 16, 4), np.uint32)
         bend_f = 2.0 ** (rng.uniform(-2, 2, (tiles, 16)) / 12.0)
+        bend_f = np.where(rng.random((tiles, 16)) < bend_prob, bend_f, 1.0)
         chan_rows[:, :, 0] = np.round(bend_f * (1 << 24)).astype(np.uint32)
         chan_rows[:, :, 1] = rng.uniform(0.2, 1.4, (tiles, 16)).astype(np.float32).view(np.uint32)
         chan_rows[:, :, 2] = rng.uniform(0.2, 1.4, (tiles, 16)).astype(np.float32).view(np.uint32)

@@ -76,6 +76,18 @@ def test_parity_unit_steps(vpl):
 
 
 @gpu
+@pytest.mark.parametrize("vpl", [1, 2])
+def test_parity_spans_broken_by_gate_rows(vpl):
+    """Unit-step voices under controller rows that mostly leave the bend at
+    unity: hot spans of up to 128 frames carry across gate tiles until a row
+    bends a channel, switches its params variant or releases a voice."""
+    sc = make_scenario(seed=17, max_voices=40000, n_blocks=4, spawn_per_block=(9000, 12000), release_rate=0.05,
+                       voices_per_lane=vpl, sort_voices=1, steps="unit", chan=True, bend_prob=0.02,
+                       block_frames=4096)
+    _compare(sc, sorted_pool=True)
+
+
+@gpu
 @pytest.mark.parametrize("interp", [N.INTERP_LINEAR, N.INTERP_NEAREST])
 def test_parity_integral_steps(interp):
     """Whole-number steps (1, 2, 3) with zero phase fractions: the
