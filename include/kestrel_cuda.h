@@ -198,6 +198,19 @@ int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n);
  * interleaved stereo floats. Blocks until the block is on the host. */
 int kc_render(kc_synth* s, float* out, size_t n);
 
+/* kc_render in two halves, so the caller can prepare the next block while
+ * this one renders: kc_render_begin enqueues the block (the staged inputs'
+ * copies, every pass, the copies back) and returns at once; kc_render_end
+ * waits for it, writes `out` and updates kc_stats. kc_render is begin then
+ * end. Between the two, kc_set_gates / kc_set_channels / kc_spawn may stage
+ * the next block (they wait only until this block's inputs have reached the
+ * device); a second begin, kc_synth_clone* and kc_batch_render are refused
+ * until end. kc_stats reports the previous block until end. No counterpart
+ * in the reference trait, whose render is synchronous. */
+int kc_render_begin(kc_synth* s);
+int kc_render_end(kc_synth* s, float* out, size_t n);
+int kc_render_pending(const kc_synth* s);
+
 /* Backend::stats (src/backend.rs:49). */
 int kc_stats(kc_synth* s, kc_block_stats* out);
 

@@ -43,6 +43,10 @@ typedef struct kh_options {
     uint32_t max_layers;            /* 16 */
     uint32_t default_channel_volume;/* 127 */
     uint32_t resample_pool;         /* 1: rebuild the pool at the output rate */
+    uint32_t read_ahead;            /* 1: the driver's event source (the synthetic
+                                       stream or the MIDI file) runs on its own
+                                       thread, ahead of the driver; the events
+                                       are the same */
     uint64_t sample_pool_budget;    /* bytes, 2 GiB */
 } kh_options;
 
@@ -189,6 +193,21 @@ int kh_driver_variant(kh_driver* d, uint32_t i, uint32_t* index, const kc_region
 /* The rest of next_block after render (src/driver.rs:619-642): returns
  * *more = 0 once the file and its tail are done. */
 int kh_driver_finish(kh_driver* d, uint64_t active_voices, int* more);
+
+/* The same two calls split for a pipelined loop, which prepares block n + 1
+ * while the backend renders block n. prepare = collect, then admit:
+ * kh_driver_collect drains the block's events (gate and controller rows,
+ * candidates, variants) and needs nothing from the backend; kh_driver_admit
+ * runs admission against `live` and fills `out`. finish = advance, then
+ * more: kh_driver_advance ends the block; kh_driver_more answers whether
+ * another block follows, from the state the last admitted block left, so it
+ * may be called after the next block's collect. The order
+ *   collect(0) admit(0) advance  [collect(n+1) more(n) admit(n+1) advance]...
+ * gives the same blocks and answers as prepare/finish. */
+int kh_driver_collect(kh_driver* d);
+int kh_driver_admit(kh_driver* d, uint32_t live, kh_block* out);
+int kh_driver_advance(kh_driver* d);
+int kh_driver_more(kh_driver* d, uint64_t active_voices, int* more);
 
 const char* kh_last_error(void);
 

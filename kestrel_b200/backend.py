@@ -101,6 +101,31 @@ class CudaSynth:
         N.check(self._lib.kc_render(self._h, N.ptr(out), out.size), self._lib)
         return out
 
+    def feed_raw(self, blk, variants) -> None:
+        """feed() from a driver block's own buffers (a KhBlock and its
+        (index, address, entries) variants), with no copies on this side."""
+        lib, h = self._lib, self._h
+        for idx, addr, n in variants:
+            N.check(lib.kc_set_params_variant(h, idx, addr, n), lib)
+        N.check(lib.kc_set_gates(h, C.cast(blk.gates, C.c_void_p), blk.n_gates), lib)
+        N.check(lib.kc_set_channels(h, C.cast(blk.chan, C.c_void_p), blk.n_chan, blk.bend, blk.gain, blk.variant),
+                lib)
+        N.check(lib.kc_spawn(h, blk.cmds if blk.n_cmds else None, blk.n_cmds), lib)
+
+    def render_begin(self) -> None:
+        """Enqueue the staged block and return; render_end collects it."""
+        N.check(self._lib.kc_render_begin(self._h), self._lib)
+
+    def render_end(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.block_frames * 2, dtype=np.float32)
+        N.check(self._lib.kc_render_end(self._h, N.ptr(out), out.size), self._lib)
+        return out
+
+    @property
+    def pending(self) -> bool:
+        return bool(self._lib.kc_render_pending(self._h))
+
     def stats(self) -> BlockStats:
         s = N.KcBlockStats()
         N.check(self._lib.kc_stats(self._h, C.byref(s)), self._lib)

@@ -612,6 +612,8 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         kc_synth* s = jobs[j];
         if (!s || !outs[j]) return fail(KC_ERR_INVALID, "null job or output at index " + std::to_string(j));
         if (!seen.insert(s).second) return fail(KC_ERR_INVALID, "job " + std::to_string(j) + " is listed twice");
+        if (s->pending)
+            return fail(KC_ERR_INVALID, "job " + std::to_string(j) + " has a block in flight (kc_render_begin)");
         if (!same_variant(b, s))
             return fail(KC_ERR_INVALID, "job " + std::to_string(j) +
                                             " differs from the batch in device, block_frames, interpolation, "

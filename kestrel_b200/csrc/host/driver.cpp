@@ -97,6 +97,7 @@ struct Driver {
     std::vector<std::pair<uint32_t, std::vector<kc_region_params>>> built;
     uint64_t notes_total = 0;
     uint32_t last_want = 0, last_take = 0, last_live = 0;
+    bool done_after_admit = false;
 
     // Driver::open, src/driver.rs:343-413.
     // The event source is the synthetic stream of `m`, or `file` when given.
@@ -111,6 +112,7 @@ struct Driver {
         bcfg.master_volume = o.master_volume;
         if (file) stream = std::move(file);
         else stream = std::make_unique<SynthMidi>(m);
+        if (o.read_ahead) stream = std::make_unique<AheadSource>(std::move(stream));
         clock = TempoClock(stream->division(), c.sample_rate);
         gates.init(c.block_frames, c.gate_frames);
         chan.init(c.block_frames, c.gate_frames);
@@ -180,7 +182,19 @@ struct Driver {
     }
 
     // next_block up to backend.spawn (src/driver.rs:434-588).
+    // Driver::next_block up to the backend's spawn is two halves: collect()
+    // drains the block's events (gate and controller rows, candidates,
+    // variants) and needs nothing from the backend; admit(live) runs
+    // admission against the backend's live count and materialises the
+    // admitted voices. Collecting block n + 1 while the device renders
+    // block n changes nothing, since collect reads only state that admit(n)
+    // has finished with.
     void prepare(uint32_t live) {
+        collect();
+        admit(live);
+    }
+
+    void collect() {
         const uint64_t block_frames = cfg.block_frames;
         const uint64_t block_start = block_index * block_frames;
         const uint64_t block_end = block_start + block_frames;
@@ -254,7 +268,9 @@ struct Driver {
         chan.end_block();
         apply_modulation();
         chan.refresh_active();
+    }
 
+    void admit(uint32_t live) {
         const uint32_t want = (uint32_t)cands.size();
         const uint32_t take = admit_take(live, want);
         last_live = live;
@@ -268,6 +284,8 @@ struct Driver {
             }
         }
         materialise(take);
+        // What finish() decides the next block by, as of this block.
+        done_after_admit = stream_done && deferred.empty();
     }
 
     // rank_candidates, src/driver.rs:701-742. select_nth_unstable is a
@@ -552,8 +570,14 @@ struct Driver {
 
     // The rest of next_block (src/driver.rs:619-642).
     bool finish(uint64_t active_voices) {
-        block_index += 1;
-        if (!stream_done || !deferred.empty()) return true;
+        advance();
+        return more(active_voices);
+    }
+    void advance() { block_index += 1; }
+    // Driver::next_block's continuation test (src/driver.rs:625-642), on the
+    // state the last admitted block left.
+    bool more(uint64_t active_voices) {
+        if (!done_after_admit) return true;
         if (active_voices > 0) {
             tail_blocks_left = tail_blocks_left > 0 ? tail_blocks_left - 1 : 0;
             return tail_blocks_left != 0;
@@ -643,6 +667,7 @@ void kh_options_default(kh_options* o) {
     o->max_layers = 16;
     o->default_channel_volume = 127;
     o->resample_pool = 1;
+    o->read_ahead = 1;
     o->sample_pool_budget = 2ull << 30;
 }
 
@@ -816,6 +841,42 @@ int kh_driver_variant(kh_driver* h, uint32_t i, uint32_t* index, const kc_region
     *index = d.built[i].first;
     *data = d.built[i].second.data();
     *n = d.built[i].second.size();
+    return 0;
+}
+
+int kh_driver_collect(kh_driver* h) {
+    h->d->collect();
+    return 0;
+}
+
+int kh_driver_admit(kh_driver* h, uint32_t live, kh_block* out) {
+    Driver& d = *h->d;
+    d.admit(live);
+    out->gates = d.gates.rows.data();
+    out->n_gates = d.gates.rows.size();
+    out->chan = d.chan.rows.data();
+    out->n_chan = d.chan.rows.size();
+    out->bend = d.chan.bend_active;
+    out->gain = d.chan.gain_active;
+    out->variant = d.chan.variant_active || d.spawn_variants;
+    out->cmds = d.spawn_buf.data();
+    out->n_cmds = d.spawn_buf.size();
+    out->n_variants = (uint32_t)d.built.size();
+    out->live = d.last_live;
+    out->want = d.last_want;
+    out->take = d.last_take;
+    out->block_index = d.block_index;
+    out->notes = d.notes_total;
+    return 0;
+}
+
+int kh_driver_advance(kh_driver* h) {
+    h->d->advance();
+    return 0;
+}
+
+int kh_driver_more(kh_driver* h, uint64_t active_voices, int* more) {
+    *more = h->d->more(active_voices) ? 1 : 0;
     return 0;
 }
 

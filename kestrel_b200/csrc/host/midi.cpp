@@ -60,6 +60,16 @@ void OffQueue::pop() {
     }
 }
 
+struct SynthMidi::WindowsAhead {
+    static constexpr size_t DEPTH = 3;
+    std::mutex m;
+    std::condition_variable produced, consumed;
+    std::deque<std::vector<On>> q;
+    std::vector<std::vector<On>> spare;
+    bool stop = false, ended = false;
+    std::thread th;
+};
+
 SynthMidi::SynthMidi(const kh_midi_spec& s)
     : spec_(s), rng_(s.seed), offs_((uint64_t)std::max(1.0, 2.0 * (double)(s.ppq ? s.ppq : 9600) / 1000.0)) {
     if (spec_.ppq == 0) spec_.ppq = 9600;
@@ -68,20 +78,121 @@ SynthMidi::SynthMidi(const kh_midi_spec& s)
     std::uniform_real_distribution<double> u(0.0, 1.0);
     phase_.resize(3 * std::max<uint32_t>(spec_.channels, 1));
     for (auto& p : phase_) p = u(rng_);
+    const bool ctrl_draws = spec_.programs > 1 && spec_.program_period_s > 0.0;
+    if (!ctrl_draws) {
+        ahead_ = std::make_unique<WindowsAhead>();
+        WindowsAhead* w = ahead_.get();
+        w->th = std::thread([this, w] {
+            for (;;) {
+                std::vector<On> v;
+                {
+                    std::unique_lock<std::mutex> g(w->m);
+                    w->consumed.wait(g, [w] { return w->stop || w->q.size() < WindowsAhead::DEPTH; });
+                    if (w->stop) return;
+                    if (!w->spare.empty()) {
+                        v = std::move(w->spare.back());
+                        w->spare.pop_back();
+                    }
+                }
+                make_window(v);
+                const bool last = v.empty();
+                {
+                    std::lock_guard<std::mutex> g(w->m);
+                    w->q.push_back(std::move(v));
+                }
+                w->produced.notify_one();
+                if (last) return;
+            }
+        });
+    }
+}
+
+SynthMidi::~SynthMidi() {
+    if (!ahead_) return;
+    {
+        std::lock_guard<std::mutex> g(ahead_->m);
+        ahead_->stop = true;
+    }
+    ahead_->consumed.notify_all();
+    ahead_->th.join();
+}
+
+// std::sort's result for a window's onset times, by a bucket sort: times
+// lie in [lo, hi) (a cluster may run up to 1 ms past hi and lands in the
+// last bucket), the bucket index is a monotone function of the time, and
+// each bucket is sorted on its own. Any correct sort of the same values
+// yields the same sequence.
+static void sort_times(std::vector<double>& v, std::vector<double>& tmp, std::vector<uint32_t>& cnt, double lo,
+                       double hi) {
+    const size_t n = v.size();
+    if (n < 64 || !(hi > lo)) {
+        std::sort(v.begin(), v.end());
+        return;
+    }
+    const size_t nb = n / 2;
+    const double scale = (double)nb / (hi - lo);
+    auto bucket = [&](double t) {
+        const double x = (t - lo) * scale;
+        const size_t i = x > 0.0 ? (size_t)x : 0;
+        return i < nb ? i : nb - 1;
+    };
+    tmp.resize(n);
+    cnt.assign(nb + 1, 0);
+    for (size_t i = 0; i < n; ++i) ++cnt[bucket(v[i]) + 1];
+    for (size_t b = 0; b < nb; ++b) cnt[b + 1] += cnt[b];
+    for (size_t i = 0; i < n; ++i) tmp[cnt[bucket(v[i])]++] = v[i];
+    size_t start = 0;  // cnt[b] is now the end of bucket b
+    for (size_t b = 0; b < nb; ++b) {
+        const size_t end = cnt[b];
+        if (end - start > 16) {
+            std::sort(tmp.begin() + (ptrdiff_t)start, tmp.begin() + (ptrdiff_t)end);
+        } else {
+            for (size_t i = start + 1; i < end; ++i) {
+                const double x = tmp[i];
+                size_t j = i;
+                for (; j > start && tmp[j - 1] > x; --j) tmp[j] = tmp[j - 1];
+                tmp[j] = x;
+            }
+        }
+        start = end;
+    }
+    v.swap(tmp);
 }
 
 void SynthMidi::refill_onsets() {
-    ons_.clear();
     on_pos_ = 0;
+    if (!ahead_) {
+        make_window(ons_);
+        return;
+    }
+    WindowsAhead* w = ahead_.get();
+    std::unique_lock<std::mutex> g(w->m);
+    if (w->ended) {
+        ons_.clear();
+        return;
+    }
+    if (ons_.capacity()) w->spare.push_back(std::move(ons_));
+    w->produced.wait(g, [w] { return !w->q.empty(); });
+    ons_ = std::move(w->q.front());
+    w->q.pop_front();
+    if (ons_.empty()) w->ended = true;
+    g.unlock();
+    w->consumed.notify_one();
+}
+
+// The next non-empty window's onsets in time order (empty at the end).
+void SynthMidi::make_window(std::vector<On>& ons) {
+    ons.clear();
     const double window = 0.25;  // seconds of onsets generated at a time
-    while (ons_.empty() && window_t_ < spec_.seconds && onsets_made_ < spec_.notes) {
+    while (ons.empty() && window_t_ < spec_.seconds && onsets_made_ < spec_.notes) {
         const double t0 = window_t_;
         const double t1 = std::min(spec_.seconds, t0 + window);
         window_t_ = t1;
         const double rate = (double)spec_.notes / std::max(spec_.seconds, 1e-9);
         const double share = std::clamp(spec_.cluster_share, 0.0, 1.0);
         const double mean_cluster = 0.5 * ((double)spec_.cluster_lo + (double)spec_.cluster_hi);
-        std::vector<double> times;
+        std::vector<double>& times = times_;
+        times.clear();
         std::poisson_distribution<uint64_t> bg((1.0 - share) * rate * (t1 - t0));
         std::uniform_real_distribution<double> ut(t0, t1);
         const uint64_t nbg = bg(rng_);
@@ -97,7 +208,7 @@ void SynthMidi::refill_onsets() {
                 for (uint32_t i = 0; i < m; ++i) times.push_back(uc(rng_));
             }
         }
-        std::sort(times.begin(), times.end());
+        sort_times(times, times_tmp_, sort_cnt_, t0, t1);
         std::uniform_int_distribution<uint32_t> uch(0, std::max<uint32_t>(spec_.channels, 1) - 1);
         std::uniform_int_distribution<uint32_t> ukey(spec_.key_lo, std::max(spec_.key_lo, spec_.key_hi));
         std::uniform_int_distribution<uint32_t> uvel(std::max<uint32_t>(spec_.vel_lo, 1),
@@ -111,7 +222,7 @@ void SynthMidi::refill_onsets() {
             o.key = (uint8_t)ukey(rng_);
             o.vel = (uint8_t)uvel(rng_);
             o.dur_s = dur(rng_);
-            ons_.push_back(o);
+            ons.push_back(o);
             ++onsets_made_;
         }
     }
@@ -221,6 +332,77 @@ bool SynthMidi::next(uint64_t* tick, Event* ev) {
     uint64_t off = tick_of((double)o.tick / ticks_per_s_ + o.dur_s);
     if (off <= o.tick) off = o.tick + 1;
     offs_.push(Off{off, off_seq_++, o.ch, o.key});  // (tick, seq) order, as pops return them
+    return true;
+}
+
+AheadSource::AheadSource(std::unique_ptr<EventSource> inner, size_t chunk, size_t depth)
+    : inner_(std::move(inner)), div_(inner_->division()), chunk_(std::max<size_t>(chunk, 1)),
+      depth_(std::max<size_t>(depth, 1)) {
+    th_ = std::thread([this] { run(); });
+}
+
+AheadSource::~AheadSource() {
+    {
+        std::lock_guard<std::mutex> g(m_);
+        stop_ = true;
+    }
+    consumed_.notify_all();
+    th_.join();
+}
+
+void AheadSource::run() {
+    for (;;) {
+        Chunk c;
+        {
+            std::unique_lock<std::mutex> g(m_);
+            consumed_.wait(g, [this] { return stop_ || q_.size() < depth_; });
+            if (stop_) return;
+            if (!spare_.empty()) {
+                c = std::move(spare_.back());
+                spare_.pop_back();
+            }
+        }
+        c.ticks.clear();
+        c.evs.clear();
+        c.last = false;
+        uint64_t tick;
+        Event ev;
+        while (c.evs.size() < chunk_) {
+            if (!inner_->next(&tick, &ev)) {
+                c.last = true;
+                break;
+            }
+            c.ticks.push_back(tick);
+            c.evs.push_back(ev);
+        }
+        const bool last = c.last;
+        {
+            std::lock_guard<std::mutex> g(m_);
+            q_.push_back(std::move(c));
+        }
+        produced_.notify_one();
+        if (last) return;
+    }
+}
+
+bool AheadSource::next(uint64_t* tick, Event* ev) {
+    while (pos_ >= cur_.evs.size()) {
+        if (ended_ || cur_.last) {
+            ended_ = true;
+            return false;
+        }
+        std::unique_lock<std::mutex> g(m_);
+        if (!cur_.evs.empty() || cur_.ticks.capacity()) spare_.push_back(std::move(cur_));
+        produced_.wait(g, [this] { return !q_.empty(); });
+        cur_ = std::move(q_.front());
+        q_.pop_front();
+        pos_ = 0;
+        g.unlock();
+        consumed_.notify_one();
+    }
+    *tick = cur_.ticks[pos_];
+    *ev = cur_.evs[pos_];
+    ++pos_;
     return true;
 }
 

@@ -4,11 +4,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <deque>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "../../../include/kestrel_host.h"
@@ -69,6 +72,40 @@ class EventSource {
     // Next event in tick order; false when the stream is exhausted.
     virtual bool next(uint64_t* tick, Event* ev) = 0;
     virtual Division division() const = 0;
+};
+
+// Another source run on its own thread, up to `depth` chunks of `chunk`
+// events ahead of the reader. The events and their order are the inner
+// source's; only the thread that produces them differs, so the driver's
+// input blocks are unchanged while generating or parsing events overlaps
+// the driver's own work.
+class AheadSource : public EventSource {
+   public:
+    AheadSource(std::unique_ptr<EventSource> inner, size_t chunk = 8192, size_t depth = 64);
+    ~AheadSource() override;
+    bool next(uint64_t* tick, Event* ev) override;
+    Division division() const override { return div_; }
+
+   private:
+    struct Chunk {
+        std::vector<uint64_t> ticks;
+        std::vector<Event> evs;
+        bool last = false;  // the inner source is exhausted after this chunk
+    };
+    void run();
+
+    std::unique_ptr<EventSource> inner_;
+    Division div_;
+    size_t chunk_, depth_;
+    std::mutex m_;
+    std::condition_variable produced_, consumed_;
+    std::deque<Chunk> q_;
+    std::vector<Chunk> spare_;  // consumed chunks handed back for reuse
+    bool stop_ = false;
+    Chunk cur_;
+    size_t pos_ = 0;
+    bool ended_ = false;
+    std::thread th_;
 };
 
 // MidiStream (src/midi.rs:239-374): a standard MIDI file read a window at a
@@ -133,6 +170,7 @@ class OffQueue {
 class SynthMidi : public EventSource {
    public:
     explicit SynthMidi(const kh_midi_spec& s);
+    ~SynthMidi() override;
     // Next event in tick order; false when the stream is exhausted.
     bool next(uint64_t* tick, Event* ev) override;
     Division division() const override {
@@ -149,6 +187,7 @@ class SynthMidi : public EventSource {
         double dur_s;
     };
     void refill_onsets();
+    void make_window(std::vector<On>& out);
     bool next_ctrl(uint64_t* tick, Event* ev, bool peek_only);
     uint64_t tick_of(double t) const { return (uint64_t)std::llround(t * ticks_per_s_); }
 
@@ -168,6 +207,14 @@ class SynthMidi : public EventSource {
     uint64_t ctrl_tick_ = 0;
     bool ctrl_done_ = false;
     std::vector<double> phase_;         // per-channel curve phases
+    std::vector<double> times_, times_tmp_;
+    std::vector<uint32_t> sort_cnt_;
+    // Onset windows made on a thread of their own, when the controller
+    // schedule never draws from rng_ (no program changes after the first):
+    // then the draws are the windows' alone and their order cannot depend
+    // on how windows and controller events interleave.
+    struct WindowsAhead;
+    std::unique_ptr<WindowsAhead> ahead_;
 };
 
 }  // namespace kh

@@ -230,6 +230,7 @@ void free_all(kc_synth* s) {
     cudaFreeHost(s->h_st);
     for (auto& e : s->ev)
         if (e) cudaEventDestroy(e);
+    if (s->ev_inputs) cudaEventDestroy(s->ev_inputs);
     for (auto& set : s->ring)
         for (auto& e : set) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -571,6 +572,7 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMallocHost(&s->h_out, samples * 4));
     KC_TRY(cudaMallocHost(&s->h_st, sizeof(DevState)));
     for (auto& e : s->ev) KC_TRY(cudaEventCreate(&e));
+    KC_TRY(cudaEventCreateWithFlags(&s->ev_inputs, cudaEventDisableTiming));
     KC_TRY(cudaDeviceSynchronize());
 #undef KC_TRY
     *out = s;
@@ -592,6 +594,7 @@ int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out) {
     if (std::memcmp(&a, &b, sizeof(a)) != 0)
         return fail(KC_ERR_INVALID, "clone config may differ from the source only in voices_per_lane and "
                                     "sort_radix_bits");
+    if (src->pending) return fail(KC_ERR_INVALID, "clone: the source has a block in flight");
     cudaSetDevice(src->device);
     KC_CUDA(cudaStreamSynchronize(src->stream));
     kc_synth* s = nullptr;
@@ -625,10 +628,23 @@ void kc_synth_destroy(kc_synth* s) {
     delete s;
 }
 
+namespace {
+// The pinned staging buffers feed the in-flight block's host-to-device
+// copies until its `ev_inputs` fires; the next block's inputs overwrite them
+// only after that.
+int staging_free(kc_synth* s) {
+    if (!s->pending) return KC_OK;
+    cudaSetDevice(s->device);
+    KC_CUDA(cudaEventSynchronize(s->ev_inputs));
+    return KC_OK;
+}
+}  // namespace
+
 int kc_set_gates(kc_synth* s, const uint32_t* rows, size_t n) {
     if (!s || (!rows && n)) return fail(KC_ERR_INVALID, "null argument");
     if (n != (size_t)s->tiles * KC_GATE_SLOTS)
         return fail(KC_ERR_INVALID, "gate rows: expected tiles * 2048 words");
+    if (int rc = staging_free(s)) return rc;
     std::memcpy(s->h_gates, rows, n * 4);
     return KC_OK;
 }
@@ -637,6 +653,7 @@ int kc_set_channels(kc_synth* s, const uint32_t* rows, size_t n, int bend, int g
     if (!s || (!rows && n)) return fail(KC_ERR_INVALID, "null argument");
     if (n != (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS)
         return fail(KC_ERR_INVALID, "channel rows: expected tiles * 64 words");
+    if (int rc = staging_free(s)) return rc;
     std::memcpy(s->h_chan, rows, n * 4);
     s->bend = bend != 0;
     s->gain = gain != 0;
@@ -667,6 +684,7 @@ int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n) {
         if (cmds[i].params >= s->params_per) return fail(KC_ERR_INVALID, "spawn command params index out of range");
         if (cmds[i].gate_slot >= KC_GATE_SLOTS) return fail(KC_ERR_INVALID, "spawn command gate_slot out of range");
     }
+    if (int rc = staging_free(s)) return rc;
     if (n > s->h_cmds_cap) {
         cudaSetDevice(s->device);
         KC_CUDA(cudaStreamSynchronize(s->stream));
@@ -684,10 +702,11 @@ int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n) {
     return KC_OK;
 }
 
-int kc_render(kc_synth* s, float* out, size_t n) {
-    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
-    const size_t samples = (size_t)s->cfg.block_frames * 2;
-    if (n != samples) return fail(KC_ERR_INVALID, "output must be block_frames * 2 samples");
+// Backend::render split at the device boundary: begin enqueues the block
+// (input copies, every pass, the copies back) and returns; end waits for it.
+int kc_render_begin(kc_synth* s) {
+    if (!s) return fail(KC_ERR_INVALID, "null synth");
+    if (s->pending) return fail(KC_ERR_INVALID, "a block is already in flight; end it first");
     cudaSetDevice(s->device);
     cudaStream_t q = s->stream;
     if (s->want > s->cmds_cap) {
@@ -701,6 +720,7 @@ int kc_render(kc_synth* s, float* out, size_t n) {
             return fail(KC_ERR_OOM, "device spawn buffer");
         s->cmds_cap = nc;
     }
+    const size_t samples = (size_t)s->cfg.block_frames * 2;
     const size_t gate_words = (size_t)s->tiles * KC_GATE_SLOTS;
     const size_t chan_words = (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS;
     KC_CUDA(cudaMemcpyAsync(s->gates, s->h_gates, gate_words * 4, cudaMemcpyHostToDevice, q));
@@ -708,13 +728,25 @@ int kc_render(kc_synth* s, float* out, size_t n) {
     if (s->want)
         KC_CUDA(cudaMemcpyAsync(s->cmds, s->h_cmds, (size_t)s->want * sizeof(kc_spawn_cmd),
                                 cudaMemcpyHostToDevice, q));
+    KC_CUDA(cudaEventRecord(s->ev_inputs, q));
     if (int rc = enqueue_block(s, s->gates, s->chan, s->bend, s->gain, s->variant, s->cmds, s->want, s->out))
         return rc;
     KC_CUDA(cudaMemcpyAsync(s->h_out, s->out, samples * 4, cudaMemcpyDeviceToHost, q));
     KC_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, q));
-    KC_CUDA(cudaStreamSynchronize(q));
-    std::memcpy(out, s->h_out, samples * 4);
     s->want = 0;
+    s->pending = true;
+    return KC_OK;
+}
+
+int kc_render_end(kc_synth* s, float* out, size_t n) {
+    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
+    const size_t samples = (size_t)s->cfg.block_frames * 2;
+    if (n != samples) return fail(KC_ERR_INVALID, "output must be block_frames * 2 samples");
+    if (!s->pending) return fail(KC_ERR_INVALID, "no block in flight");
+    cudaSetDevice(s->device);
+    KC_CUDA(cudaStreamSynchronize(s->stream));
+    s->pending = false;
+    std::memcpy(out, s->h_out, samples * 4);
     s->stats.active_voices = s->h_st->live;
     s->stats.stolen = s->h_st->stolen;
     s->stats.dropped = s->h_st->dropped;
@@ -724,6 +756,16 @@ int kc_render(kc_synth* s, float* out, size_t n) {
     if (s->h_st->error)
         return fail(KC_ERR_DEVICE, "device error word " + std::to_string(s->h_st->error));
     return KC_OK;
+}
+
+int kc_render_pending(const kc_synth* s) { return s && s->pending ? 1 : 0; }
+
+int kc_render(kc_synth* s, float* out, size_t n) {
+    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
+    const size_t samples = (size_t)s->cfg.block_frames * 2;
+    if (n != samples) return fail(KC_ERR_INVALID, "output must be block_frames * 2 samples");
+    if (int rc = kc_render_begin(s)) return rc;
+    return kc_render_end(s, out, n);
 }
 
 int kc_stats(kc_synth* s, kc_block_stats* out) {

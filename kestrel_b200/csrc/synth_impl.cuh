@@ -68,6 +68,11 @@ struct kc_synth {
 
     uint32_t want = 0;
     bool bend = false, gain = false, variant = false;
+    // A block begun with kc_render_begin and not yet ended. `ev_inputs` is
+    // recorded once the block's staged inputs have been copied to the
+    // device; the staging writers wait on it before overwriting them.
+    bool pending = false;
+    cudaEvent_t ev_inputs = nullptr;
 
     // host mirror of BlockStats
     kc_block_stats stats{};

@@ -22,7 +22,7 @@ HOST_LIB_PATH = Path(__file__).resolve().parent / "libkestrel_host.so"
 class KhOptions(C.Structure):
     _fields_ = [("master_volume", C.c_float), ("filter_enabled", C.c_uint32), ("max_layers", C.c_uint32),
                 ("default_channel_volume", C.c_uint32), ("resample_pool", C.c_uint32),
-                ("sample_pool_budget", C.c_uint64)]
+                ("read_ahead", C.c_uint32), ("sample_pool_budget", C.c_uint64)]
 
 
 class KhSynthBankSpec(C.Structure):
@@ -77,6 +77,10 @@ HOST_SYMBOLS = {
     "kh_driver_prepare": (C.c_int, [_P, C.c_uint32, C.POINTER(KhBlock)]),
     "kh_driver_variant": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "kh_driver_finish": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
+    "kh_driver_collect": (C.c_int, [_P]),
+    "kh_driver_admit": (C.c_int, [_P, C.c_uint32, C.POINTER(KhBlock)]),
+    "kh_driver_advance": (C.c_int, [_P]),
+    "kh_driver_more": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
     "kh_last_error": (C.c_char_p, []),
     "kh_gates_new": (_P, [C.c_uint32, C.c_uint32]),
     "kh_gates_destroy": (None, [_P]),
@@ -427,6 +431,45 @@ class Driver:
     def prepare(self, live: int) -> BlockInputs:
         b = KhBlock()
         self._lib.kh_driver_prepare(self._h, live, C.byref(b))
+        return self._inputs(b)
+
+    # next_block in the halves a pipelined loop calls: collect() reads the
+    # block's events and needs nothing from the backend, so it may run while
+    # the backend renders the previous block; admit(live) then needs that
+    # block's active_voices. advance() and more_after() are finish() split at
+    # the same place.
+    def collect(self) -> None:
+        self._lib.kh_driver_collect(self._h)
+
+    def admit(self, live: int) -> BlockInputs:
+        return self._inputs(self.admit_raw(live))
+
+    def admit_raw(self, live: int) -> KhBlock:
+        """admit() without copying: the block's pointers reach into the
+        driver's buffers and stay valid until the next collect()."""
+        b = KhBlock()
+        self._lib.kh_driver_admit(self._h, live, C.byref(b))
+        return b
+
+    def variant_ptrs(self, b: KhBlock) -> list[tuple[int, int, int]]:
+        """The block's params variants as (index, address, entries)."""
+        out = []
+        for i in range(b.n_variants):
+            idx, data, n = C.c_uint32(), C.c_void_p(), C.c_size_t()
+            self._lib.kh_driver_variant(self._h, i, C.byref(idx), C.byref(data), C.byref(n))
+            out.append((idx.value, data.value, n.value))
+        return out
+
+    def advance(self) -> None:
+        self._lib.kh_driver_advance(self._h)
+
+    def more_after(self, active_voices: int) -> bool:
+        more = C.c_int()
+        self._lib.kh_driver_more(self._h, active_voices, C.byref(more))
+        self.more = bool(more.value)
+        return self.more
+
+    def _inputs(self, b: KhBlock) -> BlockInputs:
         gates = np.ctypeslib.as_array(b.gates, shape=(b.n_gates,)).copy()
         chan = np.ctypeslib.as_array(b.chan, shape=(b.n_chan,)).copy()
         if b.n_cmds:

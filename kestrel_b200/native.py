@@ -133,6 +133,9 @@ CUDA_SYMBOLS = {
     "kc_set_params_variant": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t]),
     "kc_spawn": (C.c_int, [_P, _P, C.c_size_t]),
     "kc_render": (C.c_int, [_P, _P, C.c_size_t]),
+    "kc_render_begin": (C.c_int, [_P]),
+    "kc_render_end": (C.c_int, [_P, _P, C.c_size_t]),
+    "kc_render_pending": (C.c_int, [_P]),
     "kc_stats": (C.c_int, [_P, C.POINTER(KcBlockStats)]),
     "kc_name": (C.c_char_p, [_P]),
     "kc_set_profile": (C.c_int, [_P, C.c_int]),
