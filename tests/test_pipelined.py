@@ -239,3 +239,30 @@ def test_render_begin_end_contract():
     assert a.stats() == b.stats()
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("workload,over", [
+    ("steal", dict(notes=2_000_000, seconds=1.2, max_voices=50000)),
+    ("black", dict(notes=400_000, seconds=1.5, program_period_s=0.3)),
+    ("smf", {}),
+])
+def test_read_ahead_leaves_the_blocks_unchanged(tmp_path, workload, over):
+    """The event source on its own thread (and, with no program draws, the
+    onset windows on another) yields the driver the same blocks."""
+    if workload == "smf":
+        cfg, bs, _ = _spec("black")
+        ms = _sound_cc_file(tmp_path / "cc.mid")
+    else:
+        cfg, bs, ms = _spec(workload, **over)
+    bank = H.Bank(bs, cfg, H.options(read_ahead=0))
+    a = H.Driver(cfg, bank, ms)
+    bank.opt.read_ahead = 1
+    b = H.Driver(cfg, bank, ms)
+    live = 0
+    for _ in range(16):
+        x, y = a.prepare(live), b.prepare(live)
+        _same_inputs(x, y)
+        live = _decay(live, x, cfg.max_voices)
+        assert a.finish(live) == b.finish(live)
+    a.close()
+    b.close()
