@@ -10,19 +10,22 @@
  *
  *   src/bank.rs     Region/RegionParams, build_voice, make_params, the
  *                   admission preview tables, params variants
- *   src/sf2.rs      generator flattening (build_region) and build_pool
+ *   src/sf2.rs      the RIFF walk, preset/instrument flattening
+ *                   (build_region) and build_pool
  *   src/resample.rs the load-time 32-tap x 512-phase Blackman sinc
  *   src/voice.rs    GateTable, ChannelTable, admit_key/mix48/rank_gain_q
- *   src/midi.rs     TempoClock
+ *   src/midi.rs     MidiStream (standard MIDI files) and TempoClock
  *   src/driver.rs   next_block: events, admission (strata ranking),
  *                   materialise, controllers, LFO modulation
- *   src/testkit.rs  the synthetic waveforms the seeded banks are built from
+ *   src/testkit.rs  the synthetic waveforms the seeded banks are built
+ *                   from, and the SF2 writer's layout
+ *   src/limiter.rs, src/wav.rs  the output stage
  *
- * A soundfont here is described by generator lists in memory (the same
- * (operator, amount) pairs an SF2 pgen/igen chunk holds) rather than parsed
- * from a RIFF file; MIDI is a seeded synthetic event stream with the shapes
- * of the benchmark configurations. The block inputs it produces are the
- * backend's arguments verbatim: kc_spawn_cmd records, gate rows, channel rows.
+ * A soundfont is a SoundFont 2 file or a seeded synthetic bank (written in
+ * the same format and loaded by the same code); MIDI is a standard MIDI file
+ * or a seeded synthetic event stream with the shapes of the benchmark
+ * configurations. The block inputs it produces are the backend's arguments
+ * verbatim: kc_spawn_cmd records, gate rows, channel rows.
  */
 #ifndef KESTREL_HOST_H
 #define KESTREL_HOST_H
@@ -55,11 +58,12 @@ void kh_options_default(kh_options* o);
 /* ---- synthetic soundfonts ------------------------------------------------ */
 
 /* The seeded synthetic banks of the benchmark configurations: `presets`
- * presets, each one instrument of 128 zones (zone k plays key k from sample k,
+ * presets over one instrument of 128 zones (zone k plays key k from sample k,
  * root k). Sample k is `sample_frames` frames at `sample_rate` Hz: a sine at
  * the key's pitch plus white noise, looped over its last `loop_frames` frames.
  * Preset 0 uses the base envelope/filter generators below; with
- * `random_generators` every preset draws its own (seeded). */
+ * `random_generators` every other preset draws its own (seeded), held as
+ * preset-level generator offsets. */
 typedef struct kh_synth_bank_spec {
     uint32_t presets;            /* 1 or 128 */
     uint32_t sample_frames;      /* 32768 */
@@ -83,6 +87,15 @@ typedef struct kh_bank kh_bank;
 
 kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg,
                            const kh_options* opt);
+/* sf2::load (src/sf2.rs:221-505): a SoundFont 2 file. Only the samples the
+ * presets use are read; the pool is resampled to the output rate (halved
+ * until it fits options.sample_pool_budget). Null, with kh_last_error set,
+ * when the file is not a usable soundfont. The synthetic banks above are the
+ * same loader run over the bytes kh_sf2_write_synthetic writes. */
+kh_bank* kh_bank_open_sf2(const char* path, const kc_config* cfg, const kh_options* opt);
+/* The synthetic bank of `spec` as a SoundFont 2 file, in the test kit's
+ * layout (src/testkit.rs:173-318; the generate-assets step). */
+int kh_sf2_write_synthetic(const kh_synth_bank_spec* spec, const char* path);
 void kh_bank_destroy(kh_bank* b);
 /* Views into the bank; valid until kh_bank_destroy. */
 int kh_bank_pool(const kh_bank* b, const int16_t** pool, uint64_t* len);
@@ -95,6 +108,34 @@ uint32_t kh_bank_pool_rate(const kh_bank* b);
  * lowpass was designed from and whether the filter is on (make_params,
  * src/bank.rs:918-938). Each array holds kh_bank_params' length. */
 int kh_bank_filter_inputs(const kh_bank* b, float* fc_hz, float* q_cb, uint8_t* on, uint32_t n);
+
+/* What the loader made of a soundfont: bank::Region (src/bank.rs:56-160),
+ * bank::SampleInfo (src/bank.rs:34-54) and the presets' region lists. */
+typedef struct kh_region_info {
+    uint32_t sample;                /* index into the pool's samples */
+    uint8_t key_lo, key_hi, vel_lo, vel_hi;
+    int16_t root_key_override, fixed_key, fixed_vel;
+    int16_t coarse_tune, fine_tune, scale_tuning;
+    int16_t keynum_to_hold, keynum_to_decay;
+    uint8_t loop_mode;              /* 0 none, 1 continuous, 2 until release */
+    uint8_t exclusive_class;
+    float attenuation_cb, pan;
+    int32_t addr_start, addr_end, addr_loop_start, addr_loop_end;
+    float delay, attack, hold, decay, sustain, release;
+    float filter_fc_cents, filter_q_cb;
+} kh_region_info;
+typedef struct kh_sample_info {
+    uint32_t start, len, loop_start, loop_end, rate;
+    uint32_t root_key;
+    float correction_cents, resample_ratio;
+} kh_sample_info;
+uint32_t kh_bank_samples(const kh_bank* b);
+int kh_bank_region_info(const kh_bank* b, uint32_t i, kh_region_info* out);
+int kh_bank_sample_info(const kh_bank* b, uint32_t i, kh_sample_info* out);
+/* Preset i's bank and program numbers and region count; `regions` (when
+ * not null) receives up to `cap` of its region indexes. */
+int kh_bank_preset_info(const kh_bank* b, uint32_t i, uint16_t* bank, uint16_t* program,
+                        uint32_t* n_regions, uint32_t* regions, uint32_t cap);
 
 /* ---- synthetic MIDI ------------------------------------------------------ */
 

@@ -1,6 +1,6 @@
-// bank.cpp -- src/bank.rs, the flattening half of src/sf2.rs, and
-// src/resample.rs, restated in C++17. Every f32 expression is evaluated in the
-// order the Rust source writes it (the file is built with -ffp-contract=off).
+// bank.cpp -- src/bank.rs and src/resample.rs, restated in C++17. Every f32
+// expression is evaluated in the order the Rust source writes it (the file is
+// built with -ffp-contract=off).
 #include "bank.h"
 
 #include <algorithm>
@@ -483,258 +483,6 @@ std::vector<int16_t> noise(size_t n, uint64_t seed) {
         v[i] = (int16_t)((int32_t)(s >> 40) - 8192);
     }
     return v;
-}
-
-// ---- sf2.rs -------------------------------------------------------------------
-
-namespace {
-constexpr uint16_t G_START_ADDRS = 0, G_END_ADDRS = 1, G_STARTLOOP_ADDRS = 2, G_ENDLOOP_ADDRS = 3,
-                   G_START_ADDRS_COARSE = 4, G_INITIAL_FILTER_FC = 8, G_INITIAL_FILTER_Q = 9,
-                   G_END_ADDRS_COARSE = 12, G_PAN = 17, G_DELAY_VOL_ENV = 33, G_ATTACK_VOL_ENV = 34,
-                   G_HOLD_VOL_ENV = 35, G_DECAY_VOL_ENV = 36, G_SUSTAIN_VOL_ENV = 37, G_RELEASE_VOL_ENV = 38,
-                   G_KEYNUM_TO_HOLD = 39, G_KEYNUM_TO_DECAY = 40, G_INSTRUMENT = 41, G_KEY_RANGE = 43,
-                   G_VEL_RANGE = 44, G_STARTLOOP_ADDRS_COARSE = 45, G_KEYNUM = 46, G_VELOCITY = 47,
-                   G_INITIAL_ATTENUATION = 48, G_ENDLOOP_ADDRS_COARSE = 50, G_COARSE_TUNE = 51,
-                   G_FINE_TUNE = 52, G_SAMPLE_ID = 53, G_SAMPLE_MODES = 54, G_SCALE_TUNING = 56,
-                   G_EXCLUSIVE_CLASS = 57, G_OVERRIDING_ROOT_KEY = 58;
-constexpr uint32_t POOL_GUARD = 8;  // src/sf2.rs:581-583
-
-// is_absolute_only, src/sf2.rs:56-77.
-bool is_absolute_only(uint16_t op) {
-    switch (op) {
-        case G_START_ADDRS: case G_END_ADDRS: case G_STARTLOOP_ADDRS: case G_ENDLOOP_ADDRS:
-        case G_START_ADDRS_COARSE: case G_END_ADDRS_COARSE: case G_STARTLOOP_ADDRS_COARSE:
-        case G_ENDLOOP_ADDRS_COARSE: case G_SAMPLE_ID: case G_SAMPLE_MODES: case G_EXCLUSIVE_CLASS:
-        case G_OVERRIDING_ROOT_KEY: case G_KEYNUM: case G_VELOCITY: case G_INSTRUMENT: case G_KEY_RANGE:
-        case G_VEL_RANGE:
-            return true;
-        default:
-            return false;
-    }
-}
-
-// default_generators, src/sf2.rs:79-103.
-GenArray default_generators() {
-    GenArray g{};
-    g[G_INITIAL_FILTER_FC] = 13500;
-    g[21] = -12000;
-    g[23] = -12000;
-    g[25] = -12000;
-    g[26] = -12000;
-    g[27] = -12000;
-    g[28] = -12000;
-    g[30] = -12000;
-    g[G_DELAY_VOL_ENV] = -12000;
-    g[G_ATTACK_VOL_ENV] = -12000;
-    g[G_HOLD_VOL_ENV] = -12000;
-    g[G_DECAY_VOL_ENV] = -12000;
-    g[G_RELEASE_VOL_ENV] = -12000;
-    g[G_KEY_RANGE] = (int16_t)0x7F00;
-    g[G_VEL_RANGE] = (int16_t)0x7F00;
-    g[G_KEYNUM] = -1;
-    g[G_VELOCITY] = -1;
-    g[G_SCALE_TUNING] = 100;
-    g[G_OVERRIDING_ROOT_KEY] = -1;
-    return g;
-}
-
-// range_of, src/sf2.rs:508-520.
-std::pair<uint8_t, uint8_t> range_of(const GenArray& gen, bool set, uint16_t op) {
-    if (!set) return {0, 127};
-    const uint16_t raw = (uint16_t)gen[op];
-    const uint8_t lo = raw & 0xFF, hi = raw >> 8;
-    return lo > hi ? std::make_pair(hi, lo) : std::make_pair(lo, hi);
-}
-
-// build_region, src/sf2.rs:532-579.
-Region build_region(const GenArray& g, uint32_t sample, std::pair<uint8_t, uint8_t> key,
-                    std::pair<uint8_t, uint8_t> vel) {
-    Region r;
-    const float sustain_cb = (float)g[G_SUSTAIN_VOL_ENV];
-    r.sample = sample;
-    r.key_lo = key.first;
-    r.key_hi = key.second;
-    r.vel_lo = vel.first;
-    r.vel_hi = vel.second;
-    r.root_key_override = g[G_OVERRIDING_ROOT_KEY];
-    r.fixed_key = g[G_KEYNUM];
-    r.fixed_vel = g[G_VELOCITY];
-    r.coarse_tune = g[G_COARSE_TUNE];
-    r.fine_tune = g[G_FINE_TUNE];
-    r.scale_tuning = g[G_SCALE_TUNING];
-    r.attenuation_cb = (float)g[G_INITIAL_ATTENUATION];
-    r.amp_veltrack = 100.0f;
-    r.pan = rclamp((float)g[G_PAN] / 500.0f, -1.0f, 1.0f);
-    switch (g[G_SAMPLE_MODES] & 3) {
-        case 1: r.loop_mode = LoopMode::Continuous; break;
-        case 3: r.loop_mode = LoopMode::UntilRelease; break;
-        default: r.loop_mode = LoopMode::NoLoop; break;
-    }
-    r.addr_start = (int32_t)g[G_START_ADDRS] + (int32_t)g[G_START_ADDRS_COARSE] * 32768;
-    r.addr_end = (int32_t)g[G_END_ADDRS] + (int32_t)g[G_END_ADDRS_COARSE] * 32768;
-    r.addr_loop_start = (int32_t)g[G_STARTLOOP_ADDRS] + (int32_t)g[G_STARTLOOP_ADDRS_COARSE] * 32768;
-    r.addr_loop_end = (int32_t)g[G_ENDLOOP_ADDRS] + (int32_t)g[G_ENDLOOP_ADDRS_COARSE] * 32768;
-    r.exclusive_class = (uint8_t)std::clamp<int>(g[G_EXCLUSIVE_CLASS], 0, 255);
-    r.delay = timecents_to_secs((float)g[G_DELAY_VOL_ENV]);
-    r.attack = timecents_to_secs((float)g[G_ATTACK_VOL_ENV]);
-    r.hold = timecents_to_secs((float)g[G_HOLD_VOL_ENV]);
-    r.decay = timecents_to_secs((float)g[G_DECAY_VOL_ENV]);
-    r.sustain = cb_to_gain(rmax(sustain_cb, 0.0f));
-    r.release = timecents_to_secs((float)g[G_RELEASE_VOL_ENV]);
-    r.keynum_to_hold = g[G_KEYNUM_TO_HOLD];
-    r.keynum_to_decay = g[G_KEYNUM_TO_DECAY];
-    r.filter_fc_cents = (float)g[G_INITIAL_FILTER_FC];
-    r.filter_q_cb = (float)g[G_INITIAL_FILTER_Q];
-    return r;
-}
-
-int16_t sat_add16(int16_t a, int16_t b) {
-    const int32_t s = (int32_t)a + b;
-    return (int16_t)std::clamp<int32_t>(s, -32768, 32767);
-}
-}  // namespace
-
-bool load_sf2(const Sf2& sf, const BankConfig& cfg, Bank* bank, std::string* err) {
-    // ---- flatten every preset into regions (src/sf2.rs:309-467) ----
-    std::vector<Region> regions;
-    std::vector<Preset> presets;
-    std::set<uint32_t> used;
-    for (const auto& ph : sf.presets) {
-        GenArray p_gen{};
-        std::array<bool, GEN_COUNT> p_set{};
-        for (auto [op, amt] : ph.gens)
-            if (op < GEN_COUNT && op != G_INSTRUMENT) {
-                p_gen[op] = amt;
-                p_set[op] = true;
-            }
-        const auto p_key = range_of(p_gen, p_set[G_KEY_RANGE], G_KEY_RANGE);
-        const auto p_vel = range_of(p_gen, p_set[G_VEL_RANGE], G_VEL_RANGE);
-        if (ph.instrument >= sf.instruments.size()) continue;
-        std::vector<uint32_t> region_ids;
-        for (const auto& z : sf.instruments[ph.instrument]) {
-            GenArray i_gen = default_generators();
-            i_gen[G_KEY_RANGE] = (int16_t)(((uint16_t)z.key_hi << 8) | z.key_lo);
-            i_gen[G_VEL_RANGE] = (int16_t)(((uint16_t)z.vel_hi << 8) | z.vel_lo);
-            for (auto [op, amt] : z.gens)
-                if (op < GEN_COUNT && op != G_SAMPLE_ID) i_gen[op] = amt;
-            if (z.sample >= sf.samples.size()) continue;
-            const Sf2Sample& sh = sf.samples[z.sample];
-            if (sh.data.empty()) continue;
-            const auto i_key = range_of(i_gen, true, G_KEY_RANGE);
-            const auto i_vel = range_of(i_gen, true, G_VEL_RANGE);
-            const uint8_t klo = std::max(p_key.first, i_key.first), khi = std::min(p_key.second, i_key.second);
-            const uint8_t vlo = std::max(p_vel.first, i_vel.first), vhi = std::min(p_vel.second, i_vel.second);
-            if (klo > khi || vlo > vhi) continue;
-            GenArray f = i_gen;
-            for (int op = 0; op < GEN_COUNT; ++op)
-                if (p_set[op] && !is_absolute_only((uint16_t)op)) f[op] = sat_add16(f[op], p_gen[op]);
-            used.insert(z.sample);
-            region_ids.push_back((uint32_t)regions.size());
-            regions.push_back(build_region(f, z.sample, {klo, khi}, {vlo, vhi}));
-        }
-        if (!region_ids.empty()) {
-            Preset p;
-            p.bank = ph.bank;
-            p.program = ph.program;
-            p.regions = std::move(region_ids);
-            presets.push_back(std::move(p));
-        }
-    }
-    if (presets.empty()) {
-        *err = "no usable presets";
-        return false;
-    }
-
-    // ---- build_pool (src/sf2.rs:585-703) ----
-    uint32_t pool_rate = cfg.resample_pool ? cfg.sample_rate : 0;
-    if (pool_rate != 0) {
-        for (;;) {
-            uint64_t est = 0;
-            for (uint32_t sid : used) {
-                const Sf2Sample& s = sf.samples[sid];
-                const double n = (double)s.data.size() * (double)pool_rate / (double)std::max<uint32_t>(s.rate, 1);
-                est += sat_cast<uint64_t>(n) + POOL_GUARD;
-            }
-            if (est * 2 <= cfg.sample_pool_budget || pool_rate <= 8000) break;
-            pool_rate /= 2;
-        }
-    }
-    std::vector<uint32_t> remap(sf.samples.size(), UINT32_MAX);
-    Bank& b = *bank;
-    b = Bank{};
-    // With a batch resampler installed, every sample that needs converting
-    // goes to it in one call (one sinc table per distinct ratio).
-    std::unordered_map<uint32_t, std::vector<int16_t>> converted;
-    if (const ResampleHook hook = resample_hook(); hook.fn && pool_rate != 0) {
-        std::vector<uint32_t> ids, src_len, dst_len;
-        std::vector<const int16_t*> src;
-        std::vector<double> ratios;
-        std::vector<const float*> tabs;
-        std::vector<int16_t*> dst;
-        std::unordered_map<uint64_t, std::vector<float>> tables;  // by the ratio's bits
-        for (uint32_t sid : used) {
-            const Sf2Sample& sh = sf.samples[sid];
-            const uint32_t src_rate = std::max<uint32_t>(sh.rate, 1);
-            if (pool_rate == src_rate || sh.data.empty()) continue;
-            const double ratio = (double)pool_rate / (double)src_rate;
-            if (std::fabs(ratio - 1.0) < 1e-12) continue;
-            uint64_t key;
-            std::memcpy(&key, &ratio, 8);
-            auto it = tables.find(key);
-            if (it == tables.end()) it = tables.emplace(key, sinc_table(ratio)).first;
-            const size_t out_len = std::max<size_t>(sat_cast<size_t>(std::round((double)sh.data.size() * ratio)), 1);
-            auto& out = converted[sid];
-            out.resize(out_len);
-            ids.push_back(sid);
-            src.push_back(sh.data.data());
-            src_len.push_back((uint32_t)sh.data.size());
-            ratios.push_back(ratio);
-            tabs.push_back(it->second.data());
-            dst.push_back(out.data());
-            dst_len.push_back((uint32_t)out_len);
-        }
-        if (!ids.empty() && hook.fn(hook.user, (uint32_t)ids.size(), src.data(), src_len.data(), ratios.data(),
-                                    tabs.data(), dst.data(), dst_len.data()) != 0)
-            converted.clear();  // the host loop below converts them instead
-    }
-    for (uint32_t sid : used) {
-        const Sf2Sample& sh = sf.samples[sid];
-        const uint32_t src_rate = std::max<uint32_t>(sh.rate, 1);
-        uint32_t loop_start = sh.loop_start, loop_end = sh.loop_end;
-        std::vector<int16_t> data;
-        if (pool_rate != 0 && pool_rate != src_rate) {
-            const double ratio = (double)pool_rate / (double)src_rate;
-            if (auto it = converted.find(sid); it != converted.end()) data = std::move(it->second);
-            else data = resample_i16(sh.data, ratio);
-            loop_start = sat_cast<uint32_t>(std::round((double)loop_start * ratio));
-            loop_end = sat_cast<uint32_t>(std::round((double)loop_end * ratio));
-        } else {
-            data = sh.data;
-        }
-        const uint32_t len = (uint32_t)data.size();
-        loop_start = std::min(loop_start, len > 0 ? len - 1 : 0);
-        loop_end = std::min(loop_end, len);
-        SampleInfo si;
-        si.start = (uint32_t)b.pool.size();
-        b.pool.insert(b.pool.end(), data.begin(), data.end());
-        b.pool.insert(b.pool.end(), POOL_GUARD, 0);
-        si.len = len;
-        si.loop_start = loop_start;
-        si.loop_end = loop_end;
-        si.rate = pool_rate != 0 ? pool_rate : src_rate;
-        si.root_key = std::min<uint8_t>(sh.root, 127);
-        si.correction_cents = (float)sh.correction;
-        si.resample_ratio = pool_rate != 0 ? (float)pool_rate / (float)src_rate : 1.0f;
-        remap[sid] = (uint32_t)b.samples.size();
-        b.samples.push_back(si);
-    }
-    for (auto& r : regions) r.sample = r.sample < remap.size() ? remap[r.sample] : UINT32_MAX;
-    b.pool_rate = pool_rate;
-    b.regions = std::move(regions);
-    b.presets = std::move(presets);
-    b.build_params(cfg);
-    b.finish();
-    return true;
 }
 
 }  // namespace kh

@@ -146,10 +146,15 @@ struct Sf2 {
     std::vector<Sf2Preset> presets;
 };
 
-// sf2::load without the RIFF parsing: flatten presets into regions, pull the
-// used samples into the pool (resampled to the pool rate), build params and
-// the admission tables.
+// sf2::load (src/sf2.rs:221-505): walk the RIFF tree, flatten presets into
+// regions, pull the used samples into the pool (resampled to the pool rate),
+// build params and the admission tables. load_sf2 writes the in-memory
+// soundfont in the test kit's layout first, so both go through one loader.
+bool load_sf2_file(const std::string& path, const BankConfig& cfg, Bank* out, std::string* err);
 bool load_sf2(const Sf2& sf, const BankConfig& cfg, Bank* out, std::string* err);
+// Sf2Builder::write's layout (src/testkit.rs:173-318) as bytes; false when
+// the soundfont does not fit the format's indexes.
+bool write_sf2(const Sf2& sf, std::vector<uint8_t>* out, std::string* err);
 
 // resample::resample_i16 (src/resample.rs:102-107).
 std::vector<int16_t> resample_i16(const std::vector<int16_t>& src, double ratio);

@@ -614,17 +614,13 @@ Sf2 synth_sf2(const kh_synth_bank_spec& s) {
         smp.loop_end = s.sample_frames;
         sf.samples.push_back(std::move(smp));
     }
-    for (uint32_t p = 0; p < std::max<uint32_t>(s.presets, 1); ++p) {
-        int16_t attack = s.attack_tc, decay = s.decay_tc, sustain = s.sustain_cb, release = s.release_tc;
-        int16_t fc = s.filter_fc_cents, q = s.filter_q_cb;
-        if (s.random_generators && p > 0) {
-            attack = (int16_t)std::lround(-12000.0 + u(rng) * (1200.0 * std::log2(0.05) + 12000.0));
-            decay = (int16_t)std::lround(1200.0 * std::log2(0.05 + u(rng) * 1.95));
-            sustain = (int16_t)std::lround(u(rng) * 200.0);
-            release = (int16_t)std::lround(1200.0 * std::log2(0.05 + u(rng) * 0.95));
-            fc = (int16_t)std::lround(1200.0 * std::log2((1000.0 + u(rng) * 11000.0) / 8.176));
-            q = (int16_t)std::lround(u(rng) * 120.0);
-        }
+    // One instrument of 128 zones on the base generators. A preset with its
+    // own (random) generators states them as preset-level offsets, which the
+    // loader adds to the instrument's (src/sf2.rs:449-455): the flattened
+    // region holds the preset's values exactly, and the file's generator
+    // lists stay within the format's 16-bit indexes at 128 presets. An
+    // offset that would not fit 16 bits gets its own instrument instead.
+    auto instrument = [&](int16_t attack, int16_t decay, int16_t sustain, int16_t release, int16_t fc, int16_t q) {
         std::vector<Sf2Zone> inst;
         for (int k = 0; k < 128; ++k) {
             Sf2Zone z;
@@ -634,11 +630,33 @@ Sf2 synth_sf2(const kh_synth_bank_spec& s) {
             inst.push_back(std::move(z));
         }
         sf.instruments.push_back(std::move(inst));
+        return (uint16_t)(sf.instruments.size() - 1);
+    };
+    const uint16_t base = instrument(s.attack_tc, s.decay_tc, s.sustain_cb, s.release_tc, s.filter_fc_cents,
+                                     s.filter_q_cb);
+    for (uint32_t p = 0; p < std::max<uint32_t>(s.presets, 1); ++p) {
         Sf2Preset pr;
-        pr.bank = 0;
         pr.program = (uint16_t)(p % 128);
         pr.bank = (uint16_t)(p / 128);
-        pr.instrument = (uint16_t)p;
+        pr.instrument = base;
+        if (s.random_generators && p > 0) {
+            const int16_t attack = (int16_t)std::lround(-12000.0 + u(rng) * (1200.0 * std::log2(0.05) + 12000.0));
+            const int16_t decay = (int16_t)std::lround(1200.0 * std::log2(0.05 + u(rng) * 1.95));
+            const int16_t sustain = (int16_t)std::lround(u(rng) * 200.0);
+            const int16_t release = (int16_t)std::lround(1200.0 * std::log2(0.05 + u(rng) * 0.95));
+            const int16_t fc = (int16_t)std::lround(1200.0 * std::log2((1000.0 + u(rng) * 11000.0) / 8.176));
+            const int16_t q = (int16_t)std::lround(u(rng) * 120.0);
+            const std::pair<uint16_t, int32_t> offs[] = {
+                {34, attack - s.attack_tc}, {36, decay - s.decay_tc},     {37, sustain - s.sustain_cb},
+                {38, release - s.release_tc}, {8, fc - s.filter_fc_cents}, {9, q - s.filter_q_cb}};
+            bool fits = true;
+            for (auto [op, d] : offs) fits = fits && d >= -32768 && d <= 32767;
+            if (fits) {
+                for (auto [op, d] : offs) pr.gens.push_back({op, (int16_t)d});
+            } else {
+                pr.instrument = instrument(attack, decay, sustain, release, fc, q);
+            }
+        }
         sf.presets.push_back(pr);
     }
     return sf;
@@ -689,11 +707,8 @@ void kh_synth_bank_spec_default(kh_synth_bank_spec* s) {
     s->seed = 0x5EED;
 }
 
-kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg, const kh_options* opt) {
-    if (!spec || !cfg) {
-        g_err = "null argument";
-        return nullptr;
-    }
+namespace {
+BankConfig bank_config(const kc_config* cfg, const kh_options* opt) {
     kh_options o;
     kh_options_default(&o);
     if (opt) o = *opt;
@@ -706,9 +721,125 @@ kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg,
     b.master_volume = o.master_volume;
     b.resample_pool = o.resample_pool != 0;
     b.sample_pool_budget = o.sample_pool_budget;
+    return b;
+}
+}  // namespace
+
+kh_bank* kh_bank_open_sf2(const char* path, const kc_config* cfg, const kh_options* opt) {
+    if (!path || !cfg) {
+        g_err = "null argument";
+        return nullptr;
+    }
     auto* kb = new kh_bank();
-    kb->cfg = b;
-    if (!load_sf2(synth_sf2(*spec), b, &kb->bank, &g_err)) {
+    kb->cfg = bank_config(cfg, opt);
+    if (!load_sf2_file(path, kb->cfg, &kb->bank, &g_err)) {
+        delete kb;
+        return nullptr;
+    }
+    return kb;
+}
+
+int kh_sf2_write_synthetic(const kh_synth_bank_spec* spec, const char* path) {
+    if (!spec || !path) {
+        g_err = "null argument";
+        return 1;
+    }
+    std::vector<uint8_t> bytes;
+    if (!write_sf2(synth_sf2(*spec), &bytes, &g_err)) return 1;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        g_err = std::string("creating ") + path;
+        return 1;
+    }
+    const bool ok = std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size();
+    if (std::fclose(f) != 0 || !ok) {
+        g_err = std::string("writing ") + path;
+        return 1;
+    }
+    return 0;
+}
+
+uint32_t kh_bank_samples(const kh_bank* b) { return (uint32_t)b->bank.samples.size(); }
+
+int kh_bank_region_info(const kh_bank* b, uint32_t i, kh_region_info* out) {
+    if (!b || !out || i >= b->bank.regions.size()) {
+        g_err = "region index out of range";
+        return 1;
+    }
+    const Region& r = b->bank.regions[i];
+    *out = kh_region_info{};
+    out->sample = r.sample;
+    out->key_lo = r.key_lo;
+    out->key_hi = r.key_hi;
+    out->vel_lo = r.vel_lo;
+    out->vel_hi = r.vel_hi;
+    out->root_key_override = r.root_key_override;
+    out->fixed_key = r.fixed_key;
+    out->fixed_vel = r.fixed_vel;
+    out->coarse_tune = r.coarse_tune;
+    out->fine_tune = r.fine_tune;
+    out->scale_tuning = r.scale_tuning;
+    out->keynum_to_hold = r.keynum_to_hold;
+    out->keynum_to_decay = r.keynum_to_decay;
+    out->loop_mode = r.loop_mode == LoopMode::Continuous ? 1 : r.loop_mode == LoopMode::UntilRelease ? 2 : 0;
+    out->exclusive_class = r.exclusive_class;
+    out->attenuation_cb = r.attenuation_cb;
+    out->pan = r.pan;
+    out->addr_start = r.addr_start;
+    out->addr_end = r.addr_end;
+    out->addr_loop_start = r.addr_loop_start;
+    out->addr_loop_end = r.addr_loop_end;
+    out->delay = r.delay;
+    out->attack = r.attack;
+    out->hold = r.hold;
+    out->decay = r.decay;
+    out->sustain = r.sustain;
+    out->release = r.release;
+    out->filter_fc_cents = r.filter_fc_cents;
+    out->filter_q_cb = r.filter_q_cb;
+    return 0;
+}
+
+int kh_bank_sample_info(const kh_bank* b, uint32_t i, kh_sample_info* out) {
+    if (!b || !out || i >= b->bank.samples.size()) {
+        g_err = "sample index out of range";
+        return 1;
+    }
+    const SampleInfo& s = b->bank.samples[i];
+    out->start = s.start;
+    out->len = s.len;
+    out->loop_start = s.loop_start;
+    out->loop_end = s.loop_end;
+    out->rate = s.rate;
+    out->root_key = s.root_key;
+    out->correction_cents = s.correction_cents;
+    out->resample_ratio = s.resample_ratio;
+    return 0;
+}
+
+int kh_bank_preset_info(const kh_bank* b, uint32_t i, uint16_t* bank, uint16_t* program, uint32_t* n_regions,
+                        uint32_t* regions, uint32_t cap) {
+    if (!b || i >= b->bank.presets.size()) {
+        g_err = "preset index out of range";
+        return 1;
+    }
+    const Preset& p = b->bank.presets[i];
+    if (bank) *bank = p.bank;
+    if (program) *program = p.program;
+    if (n_regions) *n_regions = (uint32_t)p.regions.size();
+    if (regions)
+        for (uint32_t j = 0; j < std::min<uint32_t>(cap, (uint32_t)p.regions.size()); ++j) regions[j] = p.regions[j];
+    return 0;
+}
+
+kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg, const kh_options* opt) {
+    if (!spec || !cfg) {
+        g_err = "null argument";
+        return nullptr;
+    }
+    auto* kb = new kh_bank();
+    kb->cfg = bank_config(cfg, opt);
+    if (!load_sf2(synth_sf2(*spec), kb->cfg, &kb->bank, &g_err)) {
         delete kb;
         return nullptr;
     }

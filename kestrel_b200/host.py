@@ -49,12 +49,41 @@ class KhBlock(C.Structure):
                 ("want", C.c_uint32), ("take", C.c_uint32), ("block_index", C.c_uint64), ("notes", C.c_uint64)]
 
 
+class KhRegionInfo(C.Structure):
+    _fields_ = [("sample", C.c_uint32), ("key_lo", C.c_uint8), ("key_hi", C.c_uint8), ("vel_lo", C.c_uint8),
+                ("vel_hi", C.c_uint8), ("root_key_override", C.c_int16), ("fixed_key", C.c_int16),
+                ("fixed_vel", C.c_int16), ("coarse_tune", C.c_int16), ("fine_tune", C.c_int16),
+                ("scale_tuning", C.c_int16), ("keynum_to_hold", C.c_int16), ("keynum_to_decay", C.c_int16),
+                ("loop_mode", C.c_uint8), ("exclusive_class", C.c_uint8), ("attenuation_cb", C.c_float),
+                ("pan", C.c_float), ("addr_start", C.c_int32), ("addr_end", C.c_int32),
+                ("addr_loop_start", C.c_int32), ("addr_loop_end", C.c_int32), ("delay", C.c_float),
+                ("attack", C.c_float), ("hold", C.c_float), ("decay", C.c_float), ("sustain", C.c_float),
+                ("release", C.c_float), ("filter_fc_cents", C.c_float), ("filter_q_cb", C.c_float)]
+
+
+class KhSampleInfo(C.Structure):
+    _fields_ = [("start", C.c_uint32), ("len", C.c_uint32), ("loop_start", C.c_uint32), ("loop_end", C.c_uint32),
+                ("rate", C.c_uint32), ("root_key", C.c_uint32), ("correction_cents", C.c_float),
+                ("resample_ratio", C.c_float)]
+
+
+def _as_dict(s: C.Structure) -> dict:
+    return {name: getattr(s, name) for name, _ in s._fields_}
+
+
 _P = C.c_void_p
 HOST_SYMBOLS = {
     "kh_options_default": (None, [C.POINTER(KhOptions)]),
     "kh_synth_bank_spec_default": (None, [C.POINTER(KhSynthBankSpec)]),
     "kh_bank_synthetic": (_P, [C.POINTER(KhSynthBankSpec), C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
     "kh_bank_destroy": (None, [_P]),
+    "kh_bank_open_sf2": (_P, [C.c_char_p, C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
+    "kh_sf2_write_synthetic": (C.c_int, [C.POINTER(KhSynthBankSpec), C.c_char_p]),
+    "kh_bank_samples": (C.c_uint32, [_P]),
+    "kh_bank_region_info": (C.c_int, [_P, C.c_uint32, C.POINTER(KhRegionInfo)]),
+    "kh_bank_sample_info": (C.c_int, [_P, C.c_uint32, C.POINTER(KhSampleInfo)]),
+    "kh_bank_preset_info": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16),
+                                      C.POINTER(C.c_uint32), _P, C.c_uint32]),
     "kh_bank_pool": (C.c_int, [_P, C.POINTER(C.POINTER(C.c_int16)), C.POINTER(C.c_uint64)]),
     "kh_bank_params": (C.c_int, [_P, C.POINTER(_P), C.POINTER(C.c_uint32)]),
     "kh_bank_regions": (C.c_uint32, [_P]),
@@ -292,6 +321,12 @@ class WavWriter:
         return n.value
 
 
+def write_synthetic_sf2(spec: KhSynthBankSpec, path) -> None:
+    """The synthetic bank of `spec` as a SoundFont 2 file."""
+    if lib().kh_sf2_write_synthetic(C.byref(spec), str(path).encode()) != 0:
+        raise OSError(lib().kh_last_error().decode())
+
+
 def sinc_table(ratio: float) -> np.ndarray:
     """SincBank::new's 512 x 32 f32 table for a ratio (phase-major)."""
     t = np.empty(512 * 32, np.float32)
@@ -347,12 +382,16 @@ def midi_spec(**kw) -> KhMidiSpec:
 
 
 class Bank:
-    """A loaded bank: the i16 sample pool and the variant-0 params table."""
+    """A loaded bank: the i16 sample pool and the variant-0 params table.
+    `spec` is a synthetic bank spec or the path of a SoundFont 2 file."""
 
-    def __init__(self, spec: KhSynthBankSpec, cfg: N.KcConfig, opt: KhOptions | None = None):
+    def __init__(self, spec, cfg: N.KcConfig, opt: KhOptions | None = None):
         self._lib = lib()
         self.opt = opt or options()
-        h = self._lib.kh_bank_synthetic(C.byref(spec), C.byref(cfg), C.byref(self.opt))
+        if isinstance(spec, KhSynthBankSpec):
+            h = self._lib.kh_bank_synthetic(C.byref(spec), C.byref(cfg), C.byref(self.opt))
+        else:
+            h = self._lib.kh_bank_open_sf2(str(spec).encode(), C.byref(cfg), C.byref(self.opt))
         if not h:
             raise RuntimeError(self._lib.kh_last_error().decode())
         self._h = h
@@ -369,6 +408,31 @@ class Bank:
         self.presets = self._lib.kh_bank_presets(h)
         self.max_sample_len = self._lib.kh_bank_max_sample_len(h)
         self.pool_rate = self._lib.kh_bank_pool_rate(h)
+
+    @property
+    def n_samples(self) -> int:
+        return self._lib.kh_bank_samples(self._h)
+
+    def region_info(self, i: int) -> dict:
+        r = KhRegionInfo()
+        if self._lib.kh_bank_region_info(self._h, i, C.byref(r)) != 0:
+            raise IndexError(self._lib.kh_last_error().decode())
+        return _as_dict(r)
+
+    def sample_info(self, i: int) -> dict:
+        s = KhSampleInfo()
+        if self._lib.kh_bank_sample_info(self._h, i, C.byref(s)) != 0:
+            raise IndexError(self._lib.kh_last_error().decode())
+        return _as_dict(s)
+
+    def preset_info(self, i: int) -> tuple[int, int, list[int]]:
+        """(bank, program, region indexes) of preset i."""
+        bank, prog, n = C.c_uint16(), C.c_uint16(), C.c_uint32()
+        if self._lib.kh_bank_preset_info(self._h, i, C.byref(bank), C.byref(prog), C.byref(n), None, 0) != 0:
+            raise IndexError(self._lib.kh_last_error().decode())
+        regs = (C.c_uint32 * max(n.value, 1))()
+        self._lib.kh_bank_preset_info(self._h, i, None, None, None, regs, n.value)
+        return bank.value, prog.value, list(regs[:n.value])
 
     def filter_inputs(self):
         """(cutoff Hz, Q cB, on) per variant-0 params entry."""

@@ -1,7 +1,8 @@
 """Render a workload to a WAV file: the reference's render loop end to end.
 
-    python -m kestrel_b200.render --workload plain --out plain.wav [--midi FILE.mid]
+    python -m kestrel_b200.render --workload plain --out plain.wav [--midi FILE.mid] [--sf2 FILE.sf2]
         [--limiter brickwall|omni|off] [--format float32|pcm16] [--seconds S]
+    python -m kestrel_b200.render --workload black --write-sf2 black.sf2 [--write-midi black.mid]
 
 The loop of src/bin/kestrel.rs:311-365 around Driver::next_block
 (src/driver.rs:434-642): the driver prepares the block's inputs and hands
@@ -159,7 +160,10 @@ def main(argv=None) -> int:
     ap.add_argument("--workload", choices=["plain", "black", "steal"], default="plain")
     ap.add_argument("--midi", default=None, help="a standard MIDI file to render instead of the workload's stream")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--sf2", default=None, help="a SoundFont 2 file to render with instead of the workload's bank")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--write-sf2", default=None, help="write the workload's synthetic bank as a .sf2 file and exit")
+    ap.add_argument("--write-midi", default=None, help="write the workload's synthetic stream as a .mid file and exit")
     ap.add_argument("--limiter", choices=["brickwall", "omni", "off"], default="brickwall")
     ap.add_argument("--format", choices=["float32", "pcm16"], default="float32")
     ap.add_argument("--seconds", type=float, default=0.0, help="stop after this much audio (0: the whole file)")
@@ -167,8 +171,18 @@ def main(argv=None) -> int:
     ap.add_argument("--no-read-ahead", action="store_true", help="read MIDI events on the driver's thread")
     args = ap.parse_args(argv)
     cfg, bs, ms = H.config_workload(args.workload, seed=args.seed)
+    if args.write_sf2 or args.write_midi:
+        if args.write_sf2:
+            H.write_synthetic_sf2(bs, args.write_sf2)
+        if args.write_midi:
+            H.write_synthetic_midi(ms, args.write_midi)
+        return 0
+    if not args.out:
+        ap.error("--out is required to render")
     if args.midi:
         ms = args.midi
+    if args.sf2:
+        bs = args.sf2
     mode = {"brickwall": H.LIMITER_BRICKWALL, "omni": H.LIMITER_OMNI, "off": H.LIMITER_OFF}[args.limiter]
     fmt = H.WAV_FLOAT32 if args.format == "float32" else H.WAV_PCM16
     opt = H.options(read_ahead=0 if args.no_read_ahead else 1)
