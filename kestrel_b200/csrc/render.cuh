@@ -452,6 +452,17 @@ constexpr uint32_t RENDER_WARPS = 8;        // warps per CTA
 constexpr uint32_t SM_ROW = 72;             // floats per frame row
 constexpr uint32_t SM_HALF = 36;            // offset of lanes 16-31 in a row
 constexpr uint32_t SM_WARP = MIX_TILE * SM_ROW;   // floats per warp tile
+// The factored tile (one voice per lane, f32 tree mix): a lane stores its
+// voice's sample alone, one 32-bit store per frame into a 36-float row, and
+// its two gains once per tile; the fold multiplies by the gains. Half the
+// shared-memory traffic of the pair tile, and the per-frame gain multiplies
+// leave the voice loop. Lane l's fold reads row l >> 1 (both lanes of a row
+// read the same words, a broadcast) and gain row l & 1; rows start on 4-bank
+// steps ((36 * row) mod 32 = 4 * row), so 8 rows are one wavefront.
+constexpr uint32_t SMY_ROW = 36;            // floats per frame row
+constexpr uint32_t SMG_OFF = MIX_TILE * SMY_ROW;  // the two gain rows
+constexpr uint32_t SMG_ROW = 36;
+static_assert(SMG_OFF + 2 * SMG_ROW <= SM_WARP, "the factored tile fits the pair tile's space");
 
 // Load one voice's state into registers (the reference loads the same fields,
 // shaders/render.wgsl:203-237).
@@ -607,6 +618,25 @@ __device__ __forceinline__ void put_pair(float* sm, uint32_t lane, uint32_t i, f
     *reinterpret_cast<float2*>(sm + i * SM_ROW + (lane >> 4) * SM_HALF + (lane & 15u) * 2u) = make_float2(yl, yr);
 }
 
+// Frame i's output of this lane from its voices' samples y[k]: the sample
+// itself in a factored tile, else the gained pair, voices summed in k order.
+template <bool FACTOR, bool STRICT, int V>
+__device__ __forceinline__ void emit(float* sm, uint32_t lane, uint32_t i, const float (&y)[V],
+                                     const VoiceRegs (&v)[V]) {
+    if constexpr (FACTOR) {
+        static_assert(V == 1, "a factored tile holds one voice per lane");
+        sm[i * SMY_ROW + lane] = y[0];
+    } else {
+        float yl, yr;
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            if (k == 0) acc_out<STRICT, true>(yl, yr, y[k], v[k]);
+            else acc_out<STRICT, false>(yl, yr, y[k], v[k]);
+        }
+        put_pair(sm, lane, i, yl, yr);
+    }
+}
+
 template <bool STRICT, int FM>
 __device__ __forceinline__ float biquad_fm(VoiceRegs& v, float x) {
     if (FM == FM_NONE) return x;
@@ -646,7 +676,7 @@ struct Taps<false> {
 //  P_HOT   fractional phases: two taps and the lerp, the 32.32 phase per frame.
 // fast_ok proved every tap in bounds and phase + 16 * step free of overflow,
 // so P_UNIT and P_INT write the phase back once at the end of the tile.
-template <int KIND, int FM, bool STRICT, bool F32, int V>
+template <int KIND, int FM, bool STRICT, bool F32, int V, bool FACTOR>
 __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V], float* sm,
                                          uint32_t lane) {
     if constexpr (KIND == P_UNIT) {
@@ -655,15 +685,13 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
         for (int k = 0; k < V; ++k) t[k] = Taps<F32>(a, v[k].base + (uint32_t)(v[k].phase >> 32));
 #pragma unroll
         for (uint32_t i = 0; i < MIX_TILE; ++i) {
-            float yl, yr;
+            float y[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
-                const float y = biquad_fm<STRICT, FM>(v[k], __fmul_rn(t[k][i], v[k].level));
-                if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
-                else acc_out<STRICT, false>(yl, yr, y, v[k]);
+                y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(t[k][i], v[k].level));
             }
-            put_pair(sm, lane, i, yl, yr);
+            emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
         // 16 frames of step 1.0 (a neutral lane's step is 0)
 #pragma unroll
@@ -674,47 +702,43 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
         for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
 #pragma unroll
         for (uint32_t i = 0; i < MIX_TILE; ++i) {
-            float yl, yr;
+            float y[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
-                const float y = biquad_fm<STRICT, FM>(v[k], __fmul_rn(tap<F32>(a, off[k]), v[k].level));
+                y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(tap<F32>(a, off[k]), v[k].level));
                 off[k] += (uint32_t)(v[k].step >> 32);
-                if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
-                else acc_out<STRICT, false>(yl, yr, y, v[k]);
             }
-            put_pair(sm, lane, i, yl, yr);
+            emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
 #pragma unroll
         for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
     } else {
 #pragma unroll
         for (uint32_t i = 0; i < MIX_TILE; ++i) {
-            float yl, yr;
+            float y[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
                 const uint32_t i0 = v[k].base + (uint32_t)(v[k].phase >> 32);
                 const Taps<F32> t(a, i0);
                 const float frac = __fmul_rn(__uint2float_rn((uint32_t)v[k].phase), 2.3283064365386963e-10f);
-                const float y = biquad_fm<STRICT, FM>(v[k], __fmul_rn(lerp<STRICT>(t[0], t[1], frac), v[k].level));
+                y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(lerp<STRICT>(t[0], t[1], frac), v[k].level));
                 v[k].phase += v[k].step;
-                if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
-                else acc_out<STRICT, false>(yl, yr, y, v[k]);
             }
-            put_pair(sm, lane, i, yl, yr);
+            emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
     }
 }
 
 // Run a hot tile of kind `path` (P_UNIT, P_INT or, for linear
 // interpolation, P_HOT) with filter mode FM.
-template <int INTERP, int FM, bool STRICT, bool F32, int V>
+template <int INTERP, int FM, bool STRICT, bool F32, int V, bool FACTOR>
 __device__ __forceinline__ void hot_dispatch(int path, VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V],
                                              float* sm, uint32_t lane) {
-    if (path == P_UNIT) hot_tile<P_UNIT, FM, STRICT, F32, V>(v, a, e, sm, lane);
-    else if (path == P_INT) hot_tile<P_INT, FM, STRICT, F32, V>(v, a, e, sm, lane);
-    else if constexpr (INTERP == KC_INTERP_LINEAR) hot_tile<P_HOT, FM, STRICT, F32, V>(v, a, e, sm, lane);
+    if (path == P_UNIT) hot_tile<P_UNIT, FM, STRICT, F32, V, FACTOR>(v, a, e, sm, lane);
+    else if (path == P_INT) hot_tile<P_INT, FM, STRICT, F32, V, FACTOR>(v, a, e, sm, lane);
+    else if constexpr (INTERP == KC_INTERP_LINEAR) hot_tile<P_HOT, FM, STRICT, F32, V, FACTOR>(v, a, e, sm, lane);
 }
 
 // Render every batch of 32*V voices this warp owns. Lane l of batch b holds
@@ -724,6 +748,7 @@ __device__ __forceinline__ void hot_dispatch(int path, VoiceRegs (&v)[V], const 
 template <int INTERP, bool CHAN, bool STRICT, int MIX, int V, bool F32 = true>
 __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, uint32_t gw, uint32_t tw, uint32_t n) {
     const uint32_t lane = lane_id();
+    constexpr bool FACTOR = V == 1 && MIX == KC_MIX_F32_TREE;
     const uint32_t per = 32u * V;
     const uint32_t nbatch = (n + per - 1u) / per;
     const uint32_t samples = a.block_frames * 2u;
@@ -797,9 +822,15 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 carried = path;
             }
             if (path <= P_HOT) {
-                if (fm == FM_ALL) hot_dispatch<INTERP, FM_ALL, STRICT, F32, V>(path, v, a, e, sm, lane);
-                else if (fm == FM_NONE) hot_dispatch<INTERP, FM_NONE, STRICT, F32, V>(path, v, a, e, sm, lane);
-                else hot_dispatch<INTERP, FM_LANE, STRICT, F32, V>(path, v, a, e, sm, lane);
+                if (fm == FM_ALL) hot_dispatch<INTERP, FM_ALL, STRICT, F32, V, FACTOR>(path, v, a, e, sm, lane);
+                else if (fm == FM_NONE) hot_dispatch<INTERP, FM_NONE, STRICT, F32, V, FACTOR>(path, v, a, e, sm, lane);
+                else hot_dispatch<INTERP, FM_LANE, STRICT, F32, V, FACTOR>(path, v, a, e, sm, lane);
+            } else if (INTERP == KC_INTERP_LINEAR && path == P_FAST && FACTOR) {
+#pragma unroll
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    const float y = active[0] ? fast_frame<STRICT, F32>(v[0], a, e[0], active[0]) : 0.0f;
+                    sm[i * SMY_ROW + lane] = y;
+                }
             } else if (INTERP == KC_INTERP_LINEAR && path == P_FAST) {
 #pragma unroll
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
@@ -813,6 +844,15 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                         }
                     }
                     put_pair(sm, lane, i, yl, yr);
+                }
+            } else if (FACTOR) {
+#pragma unroll 1
+                for (uint32_t i = 0; i < MIX_TILE; ++i) {
+                    const uint32_t f = f0 + i;
+                    float y = 0.0f;
+                    if (v[0].stage != ENV_DEAD && f >= v[0].start_rel)
+                        y = voice_frame<INTERP, STRICT, F32>(v[0], a, f, looping[0]);
+                    sm[i * SMY_ROW + lane] = y;
                 }
             } else {
 #pragma unroll 1
@@ -830,10 +870,38 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                     put_pair(sm, lane, i, yl, yr);
                 }
             }
-            __syncwarp();
             // Lane l owns output slot l of the tile: frame l >> 1, channel
             // l & 1, summed over the warp's 32 lanes.
             const uint32_t h = lane & 1u;
+            if constexpr (FACTOR) {
+                // The gains hold for the whole tile (only a gate row changes
+                // them). Slot = sum over lanes of sample x gain, as four
+                // chains of eight products in lane order, then a pair tree.
+                sm[SMG_OFF + lane] = v[0].gl;
+                sm[SMG_OFF + SMG_ROW + lane] = v[0].gr;
+                __syncwarp();
+                const float4* y4 = reinterpret_cast<const float4*>(sm + (lane >> 1) * SMY_ROW);
+                const float4* g4 = reinterpret_cast<const float4*>(sm + SMG_OFF + h * SMG_ROW);
+                float s[2];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    float t = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float4 yq = y4[4 * c + q], gq = g4[4 * c + q];
+                        t = q ? __fmaf_rn(yq.x, gq.x, t) : __fmul_rn(yq.x, gq.x);
+                        t = __fmaf_rn(yq.y, gq.y, t);
+                        t = __fmaf_rn(yq.z, gq.z, t);
+                        t = __fmaf_rn(yq.w, gq.w, t);
+                    }
+                    s[c] = t;
+                }
+                __syncwarp();
+                const float sum = __fadd_rn(s[0], s[1]);
+                part[j] = first ? sum : __fadd_rn(part_prev, sum);
+                continue;
+            }
+            __syncwarp();
             const float* row = sm + (lane >> 1) * SM_ROW;
             if (MIX == KC_MIX_F32_TREE) {
                 // Half h of the row: lanes 16h..16h+15, two lanes per float4.
