@@ -22,10 +22,12 @@
 // Bit-exactness: the envelope, the steal-key inputs and the 32.32 phase are
 // computed with explicitly rounded intrinsics (__fadd_rn/__fmul_rn), which can
 // never be contracted into an FMA, statement for statement as src/cpu.rs:
-// 403-613 orders them. With STRICT the interpolation, biquad, fade and stereo
-// gain are written the same way, so each voice's per-frame contribution is
-// bit-identical to the CPU restatement's f32 value and only the summation
-// order of the mix differs.
+// 403-613 orders them. With STRICT the interpolation, biquad and fade are
+// written the same way, so each voice's per-frame sample is bit-identical to
+// the CPU restatement's f32 value; the stereo gain is a rounded product too,
+// except in the factored tile (one voice per lane, f32 tree), whose fold
+// fuses each gain product into the sum. Only the mix's summation (its order,
+// and there its rounding) differs from the CPU's.
 #pragma once
 
 #include <cstdint>
