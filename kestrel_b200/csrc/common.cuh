@@ -82,7 +82,9 @@ struct DevState {
     uint64_t dropped;      // cumulative
     uint32_t peak_bits;    // max |out| of the block, as f32 bits
     uint32_t active_warps; // render warps that own at least one voice
-    uint32_t pad[4];
+    uint32_t unit_tiles;   // warp-tiles the render ran on the unit or integral-step path
+    uint32_t all_tiles;    // warp-tiles the render ran
+    uint32_t pad[2];
 };
 
 // 64-bit step scaled by an 8.24 factor, truncating, saturating

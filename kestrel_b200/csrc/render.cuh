@@ -453,7 +453,6 @@ constexpr uint32_t RENDER_WARPS = 8;        // warps per CTA
 // ((72 * row + 36 * half) mod 32 = 8 * row + 4 * half).
 constexpr uint32_t SM_ROW = 72;             // floats per frame row
 constexpr uint32_t SM_HALF = 36;            // offset of lanes 16-31 in a row
-constexpr uint32_t SM_WARP = MIX_TILE * SM_ROW;   // floats per warp tile
 // The factored tile (one voice per lane, f32 tree mix): a lane stores its
 // voice's sample alone, one 32-bit store per frame into a 36-float row, and
 // its two gains once per tile; the fold multiplies by the gains. Half the
@@ -461,10 +460,14 @@ constexpr uint32_t SM_WARP = MIX_TILE * SM_ROW;   // floats per warp tile
 // leave the voice loop. Lane l's fold reads row l >> 1 (both lanes of a row
 // read the same words, a broadcast) and gain row l & 1; rows start on 4-bank
 // steps ((36 * row) mod 32 = 4 * row), so 8 rows are one wavefront.
+// Inside a carried span, two unit or integral-step tiles with no gate row
+// between them run as one 32-frame tile: 32 rows, one gain store and load for
+// both halves, and half the per-tile dispatch.
 constexpr uint32_t SMY_ROW = 36;            // floats per frame row
-constexpr uint32_t SMG_OFF = MIX_TILE * SMY_ROW;  // the two gain rows
+constexpr uint32_t SMG_OFF = 2 * MIX_TILE * SMY_ROW;  // the two gain rows
 constexpr uint32_t SMG_ROW = 36;
-static_assert(SMG_OFF + 2 * SMG_ROW <= SM_WARP, "the factored tile fits the pair tile's space");
+constexpr uint32_t SM_WARP = SMG_OFF + 2 * SMG_ROW;   // floats per warp
+static_assert(MIX_TILE * SM_ROW <= SM_WARP, "the pair tile fits the warp's space");
 
 // Load one voice's state into registers (the reference loads the same fields,
 // shaders/render.wgsl:203-237).
@@ -678,15 +681,17 @@ struct Taps<false> {
 //  P_HOT   fractional phases: two taps and the lerp, the 32.32 phase per frame.
 // fast_ok proved every tap in bounds and phase + 16 * step free of overflow,
 // so P_UNIT and P_INT write the phase back once at the end of the tile.
-template <int KIND, int FM, bool STRICT, bool F32, int V, bool FACTOR>
+template <int KIND, int FM, bool STRICT, bool F32, int V, bool FACTOR, uint32_t NT = MIX_TILE>
 __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V], float* sm,
                                          uint32_t lane) {
+    static_assert(NT == MIX_TILE || (NT == 2 * MIX_TILE && FACTOR), "a 32-frame tile is a factored one");
+    constexpr uint32_t LOG_NT = NT == MIX_TILE ? 4 : 5;
     if constexpr (KIND == P_UNIT) {
         Taps<F32> t[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) t[k] = Taps<F32>(a, v[k].base + (uint32_t)(v[k].phase >> 32));
 #pragma unroll
-        for (uint32_t i = 0; i < MIX_TILE; ++i) {
+        for (uint32_t i = 0; i < NT; ++i) {
             float y[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
@@ -695,15 +700,15 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
             }
             emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
-        // 16 frames of step 1.0 (a neutral lane's step is 0)
+        // NT frames of step 1.0 (a neutral lane's step is 0)
 #pragma unroll
-        for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
+        for (int k = 0; k < V; ++k) v[k].phase += v[k].step << LOG_NT;
     } else if constexpr (KIND == P_INT) {
         uint32_t off[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) off[k] = v[k].base + (uint32_t)(v[k].phase >> 32);
 #pragma unroll
-        for (uint32_t i = 0; i < MIX_TILE; ++i) {
+        for (uint32_t i = 0; i < NT; ++i) {
             float y[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
@@ -714,10 +719,10 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
             emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
 #pragma unroll
-        for (int k = 0; k < V; ++k) v[k].phase += v[k].step << 4;
+        for (int k = 0; k < V; ++k) v[k].phase += v[k].step << LOG_NT;
     } else {
 #pragma unroll
-        for (uint32_t i = 0; i < MIX_TILE; ++i) {
+        for (uint32_t i = 0; i < NT; ++i) {
             float y[V];
 #pragma unroll
             for (int k = 0; k < V; ++k) {
@@ -735,22 +740,33 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
 
 // Run a hot tile of kind `path` (P_UNIT, P_INT or, for linear
 // interpolation, P_HOT) with filter mode FM.
-template <int INTERP, int FM, bool STRICT, bool F32, int V, bool FACTOR>
+template <int INTERP, int FM, bool STRICT, bool F32, int V, bool FACTOR, uint32_t NT = MIX_TILE>
 __device__ __forceinline__ void hot_dispatch(int path, VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V],
                                              float* sm, uint32_t lane) {
-    if (path == P_UNIT) hot_tile<P_UNIT, FM, STRICT, F32, V, FACTOR>(v, a, e, sm, lane);
-    else if (path == P_INT) hot_tile<P_INT, FM, STRICT, F32, V, FACTOR>(v, a, e, sm, lane);
-    else if constexpr (INTERP == KC_INTERP_LINEAR) hot_tile<P_HOT, FM, STRICT, F32, V, FACTOR>(v, a, e, sm, lane);
+    if (path == P_UNIT) hot_tile<P_UNIT, FM, STRICT, F32, V, FACTOR, NT>(v, a, e, sm, lane);
+    else if (path == P_INT) hot_tile<P_INT, FM, STRICT, F32, V, FACTOR, NT>(v, a, e, sm, lane);
+    else if constexpr (INTERP == KC_INTERP_LINEAR && NT == MIX_TILE)
+        hot_tile<P_HOT, FM, STRICT, F32, V, FACTOR, NT>(v, a, e, sm, lane);
+}
+
+template <int INTERP, bool STRICT, bool F32, int V, bool FACTOR, uint32_t NT>
+__device__ __forceinline__ void hot_dispatch_fm(int fm, int path, VoiceRegs (&v)[V], const RenderArgs& a,
+                                                const EnvStep (&e)[V], float* sm, uint32_t lane) {
+    if (fm == FM_ALL) hot_dispatch<INTERP, FM_ALL, STRICT, F32, V, FACTOR, NT>(path, v, a, e, sm, lane);
+    else if (fm == FM_NONE) hot_dispatch<INTERP, FM_NONE, STRICT, F32, V, FACTOR, NT>(path, v, a, e, sm, lane);
+    else hot_dispatch<INTERP, FM_LANE, STRICT, F32, V, FACTOR, NT>(path, v, a, e, sm, lane);
 }
 
 // Render every batch of 32*V voices this warp owns. Lane l of batch b holds
 // voices b*32V + k*32 + l for k < V, so each of the V loads per field is one
 // coalesced line, and its V voices' frames are summed in k order before the
 // warp transpose-reduce. F32 selects the pre-converted f32 sample pool.
-template <int INTERP, bool CHAN, bool STRICT, int MIX, int V, bool F32 = true>
+template <int INTERP, bool CHAN, bool STRICT, int MIX, int V, bool F32 = true, bool DOUBLE = false>
 __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, uint32_t gw, uint32_t tw, uint32_t n) {
     const uint32_t lane = lane_id();
     constexpr bool FACTOR = V == 1 && MIX == KC_MIX_F32_TREE;
+    static_assert(!DOUBLE || FACTOR, "32-frame tiles are factored ones");
+    uint32_t unit_tiles = 0;  // tiles classified onto the unit or integral-step path
     const uint32_t per = 32u * V;
     const uint32_t nbatch = (n + per - 1u) / per;
     const uint32_t samples = a.block_frames * 2u;
@@ -782,7 +798,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
         uint32_t carry_left = 0;  // tiles of the current span still to run on `carried`
         uint32_t next_gate = 0, gt = 0;
         const bool span32 = a.gate_frames % 32u == 0u;
-        for (uint32_t f0 = 0; f0 < a.block_frames; f0 += MIX_TILE) {
+        for (uint32_t f0 = 0, nt = MIX_TILE; f0 < a.block_frames; f0 += nt) {
             if (f0 == next_gate) {
                 bool changed = false;
 #pragma unroll
@@ -822,11 +838,28 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 }
                 if (!carry_left) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e, fm);
                 carried = path;
+                if (path <= P_INT) unit_tiles += carry_left + 1u;
+            }
+            // A unit or integral-step tile whose successor is in the same
+            // span and behind no gate row runs with it as one 32-frame tile.
+            // (Fractional-step tiles stay 16 frames: doubling them measured
+            // slower.)
+            nt = MIX_TILE;
+            float part_prev2 = 0.0f;
+            if (DOUBLE && path <= P_INT && carry_left && f0 + MIX_TILE != next_gate) {
+                nt = 2u * MIX_TILE;
+                --carry_left;
+                if (!first) part_prev2 = part[j + 2u * MIX_TILE];
             }
             if (path <= P_HOT) {
-                if (fm == FM_ALL) hot_dispatch<INTERP, FM_ALL, STRICT, F32, V, FACTOR>(path, v, a, e, sm, lane);
-                else if (fm == FM_NONE) hot_dispatch<INTERP, FM_NONE, STRICT, F32, V, FACTOR>(path, v, a, e, sm, lane);
-                else hot_dispatch<INTERP, FM_LANE, STRICT, F32, V, FACTOR>(path, v, a, e, sm, lane);
+                bool done = false;
+                if constexpr (DOUBLE) {
+                    if (nt != MIX_TILE) {
+                        hot_dispatch_fm<INTERP, STRICT, F32, V, FACTOR, 2 * MIX_TILE>(fm, path, v, a, e, sm, lane);
+                        done = true;
+                    }
+                }
+                if (!done) hot_dispatch_fm<INTERP, STRICT, F32, V, FACTOR, MIX_TILE>(fm, path, v, a, e, sm, lane);
             } else if (INTERP == KC_INTERP_LINEAR && path == P_FAST && FACTOR) {
 #pragma unroll
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
@@ -884,23 +917,52 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 __syncwarp();
                 const float4* y4 = reinterpret_cast<const float4*>(sm + (lane >> 1) * SMY_ROW);
                 const float4* g4 = reinterpret_cast<const float4*>(sm + SMG_OFF + h * SMG_ROW);
-                float s[2];
+                if (!DOUBLE || nt == MIX_TILE) {
+                    float s[2];
 #pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    float t = 0.0f;
+                    for (int c = 0; c < 2; ++c) {
+                        float t = 0.0f;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float4 yq = y4[4 * c + q], gq = g4[4 * c + q];
-                        t = q ? __fmaf_rn(yq.x, gq.x, t) : __fmul_rn(yq.x, gq.x);
-                        t = __fmaf_rn(yq.y, gq.y, t);
-                        t = __fmaf_rn(yq.z, gq.z, t);
-                        t = __fmaf_rn(yq.w, gq.w, t);
+                        for (int q = 0; q < 4; ++q) {
+                            const float4 yq = y4[4 * c + q], gq = g4[4 * c + q];
+                            t = q ? __fmaf_rn(yq.x, gq.x, t) : __fmul_rn(yq.x, gq.x);
+                            t = __fmaf_rn(yq.y, gq.y, t);
+                            t = __fmaf_rn(yq.z, gq.z, t);
+                            t = __fmaf_rn(yq.w, gq.w, t);
+                        }
+                        s[c] = t;
                     }
-                    s[c] = t;
+                    __syncwarp();
+                    const float sum = __fadd_rn(s[0], s[1]);
+                    part[j] = first ? sum : __fadd_rn(part_prev, sum);
+                } else {
+                    // Slots j (frame l >> 1) and j + 32 (frame 16 + (l >> 1)),
+                    // each summed as in a 16-frame tile, sharing the gain loads.
+                    const float4* z4 = y4 + MIX_TILE * SMY_ROW / 4;
+                    float s[2], u[2];
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        float t = 0.0f, w = 0.0f;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float4 gq = g4[4 * c + q], yq = y4[4 * c + q], zq = z4[4 * c + q];
+                            t = q ? __fmaf_rn(yq.x, gq.x, t) : __fmul_rn(yq.x, gq.x);
+                            w = q ? __fmaf_rn(zq.x, gq.x, w) : __fmul_rn(zq.x, gq.x);
+                            t = __fmaf_rn(yq.y, gq.y, t);
+                            w = __fmaf_rn(zq.y, gq.y, w);
+                            t = __fmaf_rn(yq.z, gq.z, t);
+                            w = __fmaf_rn(zq.z, gq.z, w);
+                            t = __fmaf_rn(yq.w, gq.w, t);
+                            w = __fmaf_rn(zq.w, gq.w, w);
+                        }
+                        s[c] = t;
+                        u[c] = w;
+                    }
+                    __syncwarp();
+                    const float sum = __fadd_rn(s[0], s[1]), sum2 = __fadd_rn(u[0], u[1]);
+                    part[j] = first ? sum : __fadd_rn(part_prev, sum);
+                    part[j + 2u * MIX_TILE] = first ? sum2 : __fadd_rn(part_prev2, sum2);
                 }
-                __syncwarp();
-                const float sum = __fadd_rn(s[0], s[1]);
-                part[j] = first ? sum : __fadd_rn(part_prev, sum);
                 continue;
             }
             __syncwarp();
@@ -971,6 +1033,14 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
             if (vi < n) store_voice(v[k], a, vi);
         }
     }
+    // How much of the block ran on the unit or integral-step path: the host
+    // picks the next block's tile length by it (the output is the same
+    // either way).
+    if (lane == 0 && gw < nbatch) {
+        const uint32_t mine = (nbatch - gw + tw - 1u) / tw;
+        atomicAdd(&a.st->unit_tiles, unit_tiles);
+        atomicAdd(&a.st->all_tiles, mine * (a.block_frames / MIX_TILE));
+    }
 }
 
 // The render pass. Template arguments select the interpolation, whether the
@@ -979,14 +1049,14 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
 // arithmetic, and voices per lane (a per-context setting, so the summation
 // order -- and the output bits -- are a function of the config, the live
 // count and the grid alone).
-template <int INTERP, bool CHAN, bool STRICT, int MIX, int V>
+template <int INTERP, bool CHAN, bool STRICT, int MIX, int V, bool DOUBLE = false>
 __global__ void __launch_bounds__(RENDER_WARPS * 32, V == 1 ? 3 : 2)
 k_render(RenderArgs a) {
     extern __shared__ float4 smem4[];
     float* sm = reinterpret_cast<float*>(smem4) + (threadIdx.x >> 5) * SM_WARP;
     const uint32_t gw = blockIdx.x * RENDER_WARPS + (threadIdx.x >> 5);
     const uint32_t tw = gridDim.x * RENDER_WARPS;
-    render_batches<INTERP, CHAN, STRICT, MIX, V>(a, sm, gw, tw, a.st->live_render);
+    render_batches<INTERP, CHAN, STRICT, MIX, V, true, DOUBLE>(a, sm, gw, tw, a.st->live_render);
 }
 
 // Fold the warps' partial slices into the output block in a fixed order:

@@ -149,41 +149,45 @@ SortLayout plan_sort(uint32_t n_regions, uint32_t max_len) {
     return L;
 }
 
-template <int I, bool C, bool S, int M, int V>
+template <int I, bool C, bool S, int M, int V, bool D = false>
 void* render_fn() {
-    return reinterpret_cast<void*>(&k_render<I, C, S, M, V>);
+    return reinterpret_cast<void*>(&k_render<I, C, S, M, V, D>);
 }
 
 // Two voices per lane is instantiated for the linear interpolator and the
-// f32 mix only (the combinations the autotuner chooses between).
+// f32 mix only (the combinations the autotuner chooses between); so are the
+// 32-frame unit tiles (`dbl`), for one voice per lane.
 template <int I, bool C, bool S, int M>
-void* render_v(uint32_t v) {
-    if constexpr (I == KC_INTERP_LINEAR && M == KC_MIX_F32_TREE)
+void* render_v(uint32_t v, bool dbl) {
+    if constexpr (I == KC_INTERP_LINEAR && M == KC_MIX_F32_TREE) {
         if (v == 2) return render_fn<I, C, S, M, 2>();
+        if (dbl) return render_fn<I, C, S, M, 1, true>();
+    }
     return render_fn<I, C, S, M, 1>();
 }
 
 template <int I, bool C, bool S>
-void* render_m(uint32_t mix, uint32_t v) {
-    if (mix == KC_MIX_TWO_SUM) return render_v<I, C, S, KC_MIX_TWO_SUM>(v);
-    if (mix == KC_MIX_F64) return render_v<I, C, S, KC_MIX_F64>(v);
-    return render_v<I, C, S, KC_MIX_F32_TREE>(v);
+void* render_m(uint32_t mix, uint32_t v, bool dbl) {
+    if (mix == KC_MIX_TWO_SUM) return render_v<I, C, S, KC_MIX_TWO_SUM>(v, dbl);
+    if (mix == KC_MIX_F64) return render_v<I, C, S, KC_MIX_F64>(v, dbl);
+    return render_v<I, C, S, KC_MIX_F32_TREE>(v, dbl);
 }
 
 template <int I, bool C>
-void* render_sm(bool strict, uint32_t mix, uint32_t v) {
-    return strict ? render_m<I, C, true>(mix, v) : render_m<I, C, false>(mix, v);
+void* render_sm(bool strict, uint32_t mix, uint32_t v, bool dbl) {
+    return strict ? render_m<I, C, true>(mix, v, dbl) : render_m<I, C, false>(mix, v, dbl);
 }
 
-// The render instantiation for [interp][chan][strict][mix][voices per lane].
-void* render_table(uint32_t interp, bool chan, bool strict, uint32_t mix, uint32_t v) {
+// The render instantiation for [interp][chan][strict][mix][voices per
+// lane][32-frame unit tiles]. Both tile lengths give the same output bits.
+void* render_table(uint32_t interp, bool chan, bool strict, uint32_t mix, uint32_t v, bool dbl = false) {
     switch (interp) {
         case KC_INTERP_NEAREST:
-            return chan ? render_sm<0, true>(strict, mix, v) : render_sm<0, false>(strict, mix, v);
+            return chan ? render_sm<0, true>(strict, mix, v, dbl) : render_sm<0, false>(strict, mix, v, dbl);
         case KC_INTERP_LINEAR:
-            return chan ? render_sm<1, true>(strict, mix, v) : render_sm<1, false>(strict, mix, v);
+            return chan ? render_sm<1, true>(strict, mix, v, dbl) : render_sm<1, false>(strict, mix, v, dbl);
         default:
-            return chan ? render_sm<2, true>(strict, mix, v) : render_sm<2, false>(strict, mix, v);
+            return chan ? render_sm<2, true>(strict, mix, v, dbl) : render_sm<2, false>(strict, mix, v, dbl);
     }
 }
 
@@ -327,7 +331,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     ra.env_floor = c.env_floor;
     ra.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
     ra.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
-    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode, s->vpl);
+    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode, s->vpl, s->unit_tiles);
     void* args[] = {&ra};
     KC_CUDA(cudaLaunchKernel(fn, dim3(s->render_ctas), dim3(RENDER_WARPS * 32), args, s->render_smem, q));
     if (s->profile) cudaEventRecord(ev[3], q);
@@ -616,6 +620,7 @@ int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out) {
     if (e != cudaSuccess) return bail(e);
     s->parity = 0;
     s->stats = src->stats;
+    s->unit_tiles = src->unit_tiles;
     *out = s;
     return KC_OK;
 }
@@ -748,6 +753,7 @@ int kc_render_end(kc_synth* s, float* out, size_t n) {
     s->pending = false;
     std::memcpy(out, s->h_out, samples * 4);
     s->stats.active_voices = s->h_st->live;
+    if (s->h_st->all_tiles) s->unit_tiles = (uint64_t)s->h_st->unit_tiles * 2u >= s->h_st->all_tiles;
     s->stats.stolen = s->h_st->stolen;
     s->stats.dropped = s->h_st->dropped;
     uint32_t pb = s->h_st->peak_bits;
@@ -822,6 +828,7 @@ int kc_synchronize(kc_synth* s) {
     KC_CUDA(cudaStreamSynchronize(s->stream));
     drain_timings(s);
     s->stats.active_voices = s->h_st->live;
+    if (s->h_st->all_tiles) s->unit_tiles = (uint64_t)s->h_st->unit_tiles * 2u >= s->h_st->all_tiles;
     s->stats.stolen = s->h_st->stolen;
     s->stats.dropped = s->h_st->dropped;
     uint32_t pb = s->h_st->peak_bits;
