@@ -144,7 +144,11 @@ typedef struct kc_config {
     uint32_t voices_per_lane;    /* render voices per GPU lane: 0 = default (1), 1 or 2 */
     uint32_t sort_radix_bits;    /* key bits per pool-sort pass, 4..=10; 0 = default (8). The
                                     sorted order is the same for every width. */
-    uint32_t reserved[5];
+    uint32_t unit_tile_frames;   /* frames per render tile on the unit and integral-step paths
+                                    (one voice per lane, f32 tree mix): 16, 32, or 0 = chosen
+                                    per block (32 when the block before ran mostly on those
+                                    paths). The output is the same for every choice. */
+    uint32_t reserved[4];
 } kc_config;
 
 typedef struct kc_synth kc_synth;
@@ -171,7 +175,7 @@ void kc_synth_destroy(kc_synth* s);
  * forked (the benchmark forks one to replay recorded blocks from HBM). */
 int kc_synth_clone(kc_synth* src, kc_synth** out);
 /* The same, with other tunables: `cfg` must equal the source's config except
- * in voices_per_lane and sort_radix_bits, which change how a block is
+ * in voices_per_lane, sort_radix_bits and unit_tile_frames, which change how a block is
  * computed but not the voice state it leaves (voices per lane also changes
  * the summation order of the mix, within its tolerance). The autotuner times
  * its candidates on such clones of one pre-rolled context. */

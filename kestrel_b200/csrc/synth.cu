@@ -259,6 +259,8 @@ int validate(const kc_config& c) {
     if (c.voices_per_lane > 2) return fail(KC_ERR_INVALID, "voices_per_lane must be 0, 1 or 2");
     if (c.sort_radix_bits && (c.sort_radix_bits < SORT_RADIX_MIN || c.sort_radix_bits > SORT_RADIX_MAX))
         return fail(KC_ERR_INVALID, "sort_radix_bits must be 0 or in 4..=10");
+    if (c.unit_tile_frames != 0 && c.unit_tile_frames != 16 && c.unit_tile_frames != 32)
+        return fail(KC_ERR_INVALID, "unit_tile_frames must be 0, 16 or 32");
     if (c.max_param_variants == 0 || c.max_param_variants > 64)
         return fail(KC_ERR_INVALID, "max_param_variants must be in 1..=64");
     return KC_OK;
@@ -331,7 +333,8 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     ra.env_floor = c.env_floor;
     ra.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
     ra.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
-    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode, s->vpl, s->unit_tiles);
+    const bool dbl = c.unit_tile_frames == 32 || (c.unit_tile_frames == 0 && s->unit_tiles);
+    void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode, s->vpl, dbl);
     void* args[] = {&ra};
     KC_CUDA(cudaLaunchKernel(fn, dim3(s->render_ctas), dim3(RENDER_WARPS * 32), args, s->render_smem, q));
     if (s->profile) cudaEventRecord(ev[3], q);
@@ -595,9 +598,10 @@ int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out) {
     kc_config a = src->cfg, b = *cfg;
     a.voices_per_lane = b.voices_per_lane = 0;
     a.sort_radix_bits = b.sort_radix_bits = 0;
+    a.unit_tile_frames = b.unit_tile_frames = 0;
     if (std::memcmp(&a, &b, sizeof(a)) != 0)
-        return fail(KC_ERR_INVALID, "clone config may differ from the source only in voices_per_lane and "
-                                    "sort_radix_bits");
+        return fail(KC_ERR_INVALID, "clone config may differ from the source only in voices_per_lane, "
+                                    "sort_radix_bits and unit_tile_frames");
     if (src->pending) return fail(KC_ERR_INVALID, "clone: the source has a block in flight");
     cudaSetDevice(src->device);
     KC_CUDA(cudaStreamSynchronize(src->stream));

@@ -58,7 +58,8 @@ class KcConfig(C.Structure):
         ("interpolation", C.c_uint32), ("decay_curve", C.c_uint32), ("release_curve", C.c_uint32),
         ("env_floor", C.c_float), ("sort_voices", C.c_uint32), ("max_param_variants", C.c_uint32),
         ("mix_mode", C.c_uint32), ("strict_fp", C.c_uint32), ("device", C.c_uint32),
-        ("voices_per_lane", C.c_uint32), ("sort_radix_bits", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+        ("voices_per_lane", C.c_uint32), ("sort_radix_bits", C.c_uint32), ("unit_tile_frames", C.c_uint32),
+        ("reserved", C.c_uint32 * 4)]
 
 
 class KcBlockStats(C.Structure):
@@ -88,6 +89,7 @@ def default_config(**overrides) -> KcConfig:
     c.device = 0
     c.voices_per_lane = 0
     c.sort_radix_bits = 0
+    c.unit_tile_frames = 0
     for k, v in overrides.items():
         if not hasattr(c, k):
             raise AttributeError(f"kc_config has no field {k!r}")

@@ -88,7 +88,7 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
                   mix_mode=N.MIX_F32_TREE, strict_fp: int = 1, steal_percent: int = 25,
                   release_rate: float = 0.3, steps: str = "ratio", decay_curve=N.CURVE_EXPONENTIAL,
                   release_curve=N.CURVE_EXPONENTIAL, voices_per_lane: int = 0, sort_radix_bits: int = 0,
-                  bend_prob: float = 1.0) -> Scenario:
+                  bend_prob: float = 1.0, unit_tile_frames: int = 0) -> Scenario:
     """steps: "ratio" (pitch ratios 2^U(-1.5, 1.5), random phase fractions),
     "unit" (every step exactly 1.0 and every phase fraction zero: the root key
     at the pool rate) or "integral" (steps of exactly 1, 2 or 3 with zero
@@ -100,7 +100,8 @@ def make_scenario(seed: int = 1, *, max_voices: int = 4096, n_blocks: int = 6, s
                            sort_voices=sort_voices, mix_mode=mix_mode, strict_fp=strict_fp,
                            max_steal_percent=steal_percent, max_param_variants=max(variants + 1, 1),
                            decay_curve=decay_curve, release_curve=release_curve,
-                           voices_per_lane=voices_per_lane, sort_radix_bits=sort_radix_bits)
+                           voices_per_lane=voices_per_lane, sort_radix_bits=sort_radix_bits,
+                           unit_tile_frames=unit_tile_frames)
     pool, starts, params = make_bank(rng, n_samples, frames, n_params)
     tiles = block_frames // gate_frames
     on_count = np.zeros(N.GATE_SLOTS, np.uint32)

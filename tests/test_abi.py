@@ -86,7 +86,7 @@ def test_config_validation_needs_no_device():
     pool = np.zeros(16, np.int16)
     params = np.zeros(1, N.PARAMS_DTYPE)
     for bad in (dict(sort_radix_bits=3), dict(sort_radix_bits=11), dict(voices_per_lane=3),
-                dict(block_frames=1000), dict(mix_mode=7)):
+                dict(block_frames=1000), dict(mix_mode=7), dict(unit_tile_frames=24), dict(unit_tile_frames=64)):
         cfg = N.default_config(max_voices=16, **bad)
         rc = lib.kc_synth_create(C.byref(cfg), N.ptr(pool), pool.size, N.ptr(params), 1, 1, 16, C.byref(out))
         assert rc == 1, bad  # KC_ERR_INVALID

@@ -117,6 +117,30 @@ def test_sort_radix_widths_agree():
 
 
 @gpu
+@pytest.mark.parametrize("steps,chan", [("unit", True), ("integral", False), (None, True)])
+def test_unit_tile_lengths_agree(steps, chan):
+    """16-frame and 32-frame unit tiles, and the per-block choice between
+    them, leave byte-identical blocks and pools; the 32-frame form against
+    the CPU reference as well."""
+    from kestrel_b200.backend import CudaSynth
+    ref = None
+    for utf in (16, 32, 0):
+        kw = dict(steps=steps) if steps else {}
+        sc = make_scenario(seed=19, max_voices=30000, n_blocks=5, spawn_per_block=(6000, 9000), release_rate=0.03,
+                           sort_voices=1, chan=chan, bend_prob=0.02, block_frames=4096, unit_tile_frames=utf, **kw)
+        cu = CudaSynth(sc.cfg, sc.pool, sc.params, sc.n_regions, sc.max_len)
+        o, s, p, _ = run(cu, sc, collect_pool=True)
+        cu.close()
+        got = (np.concatenate(o).tobytes(), [x.tobytes() for x in p])
+        if ref is None:
+            ref = got
+        else:
+            assert got == ref, f"unit_tile_frames {utf}"
+        if utf == 32:
+            _compare(sc, sorted_pool=True)
+
+
+@gpu
 def test_parity_oldest_even_nochan():
     sc = make_scenario(seed=2, steal_rule=N.STEAL_OLDEST, admit_rule=N.ADMIT_EVEN, chan=False, variants=0)
     _compare(sc)
