@@ -1,8 +1,8 @@
 """Render a workload to a WAV file: the reference's render loop end to end.
 
-    python -m kestrel_b200.render --workload plain --out plain.wav [--midi FILE.mid] [--sf2 FILE.sf2]
-        [--limiter brickwall|omni|off] [--format float32|pcm16] [--seconds S]
-    python -m kestrel_b200.render --workload black --write-sf2 black.sf2 [--write-midi black.mid]
+    python -m kestrel_b200.render song.mid -s bank.sf2 -o out.wav [--max-voices N] [--limiter ...] ...
+    python -m kestrel_b200.render --workload plain -o plain.wav     (a seeded synthetic workload)
+    python -m kestrel_b200.render --workload black --write-sf2 black.sf2 --write-midi black.mid
 
 The loop of src/bin/kestrel.rs:311-365 around Driver::next_block
 (src/driver.rs:434-642): the driver prepares the block's inputs and hands
@@ -155,17 +155,61 @@ def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block):
             return blocks, frames, peak_voices, ph
 
 
+# The spellings each option accepts (src/config.rs:20-150).
+_INTERP = {"nearest": 0, "none": 0, "0": 0, "linear": 1, "1": 1, "cubic": 2, "hermite": 2, "2": 2}
+_CURVE = {"exp": 0, "exponential": 0, "db": 0, "lin": 1, "linear": 1}
+_STEAL = {"oldest": 0, "drop": 1, "dropnew": 1, "drop-new": 1, "quietest": 2, "quiet": 2, "level": 2}
+_ADMIT = {"loudest": 0, "loud": 0, "rank": 0, "ranked": 0, "even": 1, "spread": 1, "flat": 1}
+
+
+def _choice(table, name):
+    def parse(v):
+        key = v.lower()
+        if key not in table:
+            raise argparse.ArgumentTypeError(f"unknown {name} {v!r}")
+        return table[key]
+    return parse
+
+
 def main(argv=None) -> int:
-    ap = argparse.ArgumentParser()
+    """`kestrel render` (src/bin/kestrel.rs:72-187) with the CUDA backend:
+    MIDI file, -s soundfont.sf2, -o out.wav and the options that reach the
+    driver, the backend and the output stage. Without a MIDI file, a seeded
+    synthetic workload stands in (--workload)."""
+    ap = argparse.ArgumentParser(prog="python -m kestrel_b200.render")
+    ap.add_argument("midi", nargs="?", default=None, help="input MIDI file (default: the workload's synthetic stream)")
+    ap.add_argument("-s", "--soundfont", "--sf2", dest="soundfont", default=None,
+                    help="SoundFont 2 file (default: the workload's synthetic bank)")
+    ap.add_argument("-o", "--out", default=None, help="output WAV")
+    ap.add_argument("--midi", dest="midi_opt", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["plain", "black", "steal"], default="plain")
-    ap.add_argument("--midi", default=None, help="a standard MIDI file to render instead of the workload's stream")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--sf2", default=None, help="a SoundFont 2 file to render with instead of the workload's bank")
-    ap.add_argument("--out", default=None)
     ap.add_argument("--write-sf2", default=None, help="write the workload's synthetic bank as a .sf2 file and exit")
     ap.add_argument("--write-midi", default=None, help="write the workload's synthetic stream as a .mid file and exit")
-    ap.add_argument("--limiter", choices=["brickwall", "omni", "off"], default="brickwall")
+    ap.add_argument("--rate", type=int, default=None, help="output sample rate (48000)")
+    ap.add_argument("--block", type=int, default=None, help="frames per block (4096)")
+    ap.add_argument("--gate-frames", type=int, default=None, help="frames between note-off gate checks (32)")
+    ap.add_argument("--max-voices", type=int, default=None)
+    ap.add_argument("--layers", type=int, default=None, help="regions a note may sound (16)")
+    ap.add_argument("--interp", type=_choice(_INTERP, "interpolation"), default=None)
+    ap.add_argument("--decay-curve", type=_choice(_CURVE, "curve"), default=None)
+    ap.add_argument("--release-curve", type=_choice(_CURVE, "curve"), default=None)
+    ap.add_argument("--steal", type=_choice(_STEAL, "steal rule"), default=None)
+    ap.add_argument("--admit", type=_choice(_ADMIT, "admit rule"), default=None)
+    ap.add_argument("--steal-percent", type=int, default=None)
     ap.add_argument("--format", choices=["float32", "pcm16"], default="float32")
+    ap.add_argument("--volume", type=float, default=None, help="master volume (1.0)")
+    ap.add_argument("--no-limiter", action="store_true")
+    ap.add_argument("--limiter", choices=["brickwall", "omni", "off"], default="brickwall")
+    ap.add_argument("--ceiling-db", type=float, default=0.0)
+    ap.add_argument("--lookahead-ms", type=float, default=2.0)
+    ap.add_argument("--limiter-release-ms", type=float, default=60.0)
+    ap.add_argument("--limiter-sustain-ms", type=float, default=0.0)
+    ap.add_argument("--no-true-peak", action="store_true")
+    ap.add_argument("--no-filter", action="store_true")
+    ap.add_argument("--no-sort", action="store_true")
+    ap.add_argument("--no-resample-pool", action="store_true")
+    ap.add_argument("--pool-budget", type=int, default=2048, help="sample pool budget in MiB")
     ap.add_argument("--seconds", type=float, default=0.0, help="stop after this much audio (0: the whole file)")
     ap.add_argument("--serial", action="store_true", help="the reference's serial loop instead of the pipelined one")
     ap.add_argument("--no-read-ahead", action="store_true", help="read MIDI events on the driver's thread")
@@ -178,16 +222,34 @@ def main(argv=None) -> int:
             H.write_synthetic_midi(ms, args.write_midi)
         return 0
     if not args.out:
-        ap.error("--out is required to render")
-    if args.midi:
-        ms = args.midi
-    if args.sf2:
-        bs = args.sf2
-    mode = {"brickwall": H.LIMITER_BRICKWALL, "omni": H.LIMITER_OMNI, "off": H.LIMITER_OFF}[args.limiter]
+        ap.error("-o/--out is required to render")
+    midi = args.midi or args.midi_opt
+    if midi:
+        ms = midi
+    if args.soundfont:
+        bs = args.soundfont
+    for field, val in (("sample_rate", args.rate), ("block_frames", args.block), ("gate_frames", args.gate_frames),
+                       ("max_voices", args.max_voices), ("interpolation", args.interp),
+                       ("decay_curve", args.decay_curve), ("release_curve", args.release_curve),
+                       ("steal_rule", args.steal), ("admit_rule", args.admit),
+                       ("max_steal_percent", args.steal_percent)):
+        if val is not None:
+            setattr(cfg, field, val)
+    if args.no_sort:
+        cfg.sort_voices = 0
+    opt = H.options(read_ahead=0 if args.no_read_ahead else 1, filter_enabled=0 if args.no_filter else 1,
+                    resample_pool=0 if args.no_resample_pool else 1, sample_pool_budget=args.pool_budget << 20)
+    if args.layers is not None:
+        opt.max_layers = args.layers
+    if args.volume is not None:
+        opt.master_volume = args.volume
+    mode = H.LIMITER_OFF if args.no_limiter else \
+        {"brickwall": H.LIMITER_BRICKWALL, "omni": H.LIMITER_OMNI, "off": H.LIMITER_OFF}[args.limiter]
     fmt = H.WAV_FLOAT32 if args.format == "float32" else H.WAV_PCM16
-    opt = H.options(read_ahead=0 if args.no_read_ahead else 1)
+    lim_opts = dict(ceiling_db=args.ceiling_db, lookahead_ms=args.lookahead_ms, release_ms=args.limiter_release_ms,
+                    sustain_ms=args.limiter_sustain_ms, true_peak=not args.no_true_peak)
     st = render_file(args.out, cfg, bs, ms, limiter=mode, fmt=fmt, max_seconds=args.seconds,
-                     pipelined=False if args.serial else None, options=opt)
+                     pipelined=False if args.serial else None, options=opt, limiter_opts=lim_opts)
     print(f"{st.seconds:.2f} s rendered in {st.wall_s:.2f} s ({st.x_realtime:.2f}x realtime), {st.blocks} blocks, "
           f"peak {st.peak_voices} voices, {st.clipped} samples clipped, {st.data_bytes} bytes"
           + (", host s: " + ", ".join(f"{k} {v:.2f}" for k, v in st.phases.items()) if st.phases else ""),

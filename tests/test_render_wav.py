@@ -56,3 +56,38 @@ def test_pcm16_render(tmp_path):
     x, y = _payload(tmp_path / "a.wav", H.WAV_PCM16), _payload(tmp_path / "b.wav", H.WAV_PCM16)
     # A -100 dB null is far below one pcm16 step: the files differ by at most one code, rarely
     assert np.max(np.abs(x.astype(np.int32) - y.astype(np.int32))) <= 1
+
+
+def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
+    """`python -m kestrel_b200.render song.mid -s bank.sf2 -o out.wav ...`
+    takes `kestrel render`'s options (src/bin/kestrel.rs:72-187, spellings
+    of src/config.rs:20-150) to the config, the driver options and the
+    output stage."""
+    from kestrel_b200 import native as N
+    from kestrel_b200 import render as R
+    seen = {}
+
+    def fake(path, cfg, bank, midi, limiter, fmt, max_seconds, pipelined, options, limiter_opts):
+        seen.update(path=path, cfg=cfg, bank=bank, midi=midi, limiter=limiter, fmt=fmt, seconds=max_seconds,
+                    pipelined=pipelined, opt=options, lim=limiter_opts)
+        return R.RenderStats(1, 0.1, 0.1, 0, 0, 0, 0)
+
+    monkeypatch.setattr(R, "render_file", fake)
+    R.main(["song.mid", "-s", "bank.sf2", "-o", str(tmp_path / "o.wav"), "--rate", "44100", "--block", "2048",
+            "--max-voices", "5000", "--interp", "hermite", "--decay-curve", "lin", "--steal", "drop-new",
+            "--admit", "spread", "--steal-percent", "50", "--format", "pcm16", "--volume", "0.5", "--layers", "4",
+            "--ceiling-db", "-1", "--no-true-peak", "--no-filter", "--no-sort", "--no-resample-pool",
+            "--pool-budget", "64", "--seconds", "3", "--serial"])
+    c, o = seen["cfg"], seen["opt"]
+    assert seen["midi"] == "song.mid" and seen["bank"] == "bank.sf2"
+    assert (c.sample_rate, c.block_frames, c.max_voices, c.max_steal_percent) == (44100, 2048, 5000, 50)
+    assert (c.interpolation, c.decay_curve, c.steal_rule, c.admit_rule, c.sort_voices) == \
+        (N.INTERP_CUBIC, N.CURVE_LINEAR, N.STEAL_DROP_NEW, N.ADMIT_EVEN, 0)
+    assert (o.filter_enabled, o.resample_pool, o.sample_pool_budget, o.max_layers) == (0, 0, 64 << 20, 4)
+    assert abs(o.master_volume - 0.5) < 1e-7
+    assert seen["fmt"] == H.WAV_PCM16 and seen["seconds"] == 3.0 and seen["pipelined"] is False
+    assert seen["lim"]["ceiling_db"] == -1.0 and seen["lim"]["true_peak"] is False
+    R.main(["-o", str(tmp_path / "o.wav"), "--no-limiter"])
+    assert seen["limiter"] == H.LIMITER_OFF and seen["pipelined"] is None
+    with pytest.raises(SystemExit):
+        R.main(["x.mid", "-o", "y.wav", "--steal", "loudest"])
