@@ -93,6 +93,20 @@ kh_bank* kh_bank_synthetic(const kh_synth_bank_spec* spec, const kc_config* cfg,
  * when the file is not a usable soundfont. The synthetic banks above are the
  * same loader run over the bytes kh_sf2_write_synthetic writes. */
 kh_bank* kh_bank_open_sf2(const char* path, const kc_config* cfg, const kh_options* opt);
+/* sfz::load (src/sfz.rs:262-415): an SFZ instrument and the WAV files it
+ * names (8/16/24/32-bit PCM, 32/64-bit float; loop points, root key and
+ * tuning from the smpl chunk, src/wav.rs:160-356), as one preset. Stereo
+ * samples become two regions panned hard left and right. */
+kh_bank* kh_bank_open_sfz(const char* path, const kc_config* cfg, const kh_options* opt);
+/* load_bank (src/lib.rs:32-48): .sf2 / .sf3 / .sfbk or .sfz, by extension. */
+kh_bank* kh_bank_open(const char* path, const kc_config* cfg, const kh_options* opt);
+/* The loader's warnings, one per line (unreadable samples; unsupported SFZ
+ * opcodes with their counts); empty when there were none. */
+const char* kh_bank_report(const kh_bank* b);
+/* SFZ's note names (`c4` = 60, `c#4`, `eb3`, `c-1`); 0 when `s` is one. */
+int kh_sfz_note_name(const char* s, int32_t* out);
+/* Where an SFZ opcode value ends in the text after its `=`. */
+size_t kh_sfz_value_end(const char* s);
 /* The synthetic bank of `spec` as a SoundFont 2 file, in the test kit's
  * layout (src/testkit.rs:173-318; the generate-assets step). */
 int kh_sf2_write_synthetic(const kh_synth_bank_spec* spec, const char* path);

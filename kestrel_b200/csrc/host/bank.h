@@ -156,6 +156,15 @@ bool load_sf2(const Sf2& sf, const BankConfig& cfg, Bank* out, std::string* err)
 // the soundfont does not fit the format's indexes.
 bool write_sf2(const Sf2& sf, std::vector<uint8_t>* out, std::string* err);
 
+// sfz::load (src/sfz.rs:262-415): an SFZ instrument and the WAV files it
+// names. `report` receives the warnings (unreadable samples, unsupported
+// opcodes with their counts).
+bool load_sfz_file(const std::string& path, const BankConfig& cfg, Bank* out, std::string* err,
+                   std::vector<std::string>* report);
+// parse_note_name and find_value_end (src/sfz.rs:88-116, 233-260).
+bool sfz_note_name(const std::string& s, int32_t* out);
+size_t sfz_value_end(const std::string& s);
+
 // resample::resample_i16 (src/resample.rs:102-107).
 std::vector<int16_t> resample_i16(const std::vector<int16_t>& src, double ratio);
 // SincBank::new (src/resample.rs:18-49): 512 phases x 32 taps, phase-major.

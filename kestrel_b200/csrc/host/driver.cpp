@@ -2,6 +2,7 @@
 // admission and controller machinery, restated in C++17, plus the C ABI of
 // include/kestrel_host.h.
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -670,6 +671,7 @@ using namespace kh;
 struct kh_bank {
     Bank bank;
     BankConfig cfg;
+    std::string report;  // the loader's warnings, one per line
 };
 struct kh_driver {
     std::unique_ptr<Driver> d;
@@ -738,6 +740,44 @@ kh_bank* kh_bank_open_sf2(const char* path, const kc_config* cfg, const kh_optio
     }
     return kb;
 }
+
+kh_bank* kh_bank_open_sfz(const char* path, const kc_config* cfg, const kh_options* opt) {
+    if (!path || !cfg) {
+        g_err = "null argument";
+        return nullptr;
+    }
+    auto* kb = new kh_bank();
+    kb->cfg = bank_config(cfg, opt);
+    std::vector<std::string> report;
+    if (!load_sfz_file(path, kb->cfg, &kb->bank, &g_err, &report)) {
+        delete kb;
+        return nullptr;
+    }
+    for (const auto& line : report) kb->report += line + "\n";
+    return kb;
+}
+
+kh_bank* kh_bank_open(const char* path, const kc_config* cfg, const kh_options* opt) {
+    if (!path) {
+        g_err = "null argument";
+        return nullptr;
+    }
+    // load_bank (src/lib.rs:32-48): by the file's extension
+    std::string p = path;
+    const size_t dot = p.rfind('.');
+    const size_t slash = p.rfind('/');
+    std::string ext = dot == std::string::npos || (slash != std::string::npos && dot < slash) ? "" : p.substr(dot + 1);
+    for (auto& c : ext) c = (char)std::tolower((unsigned char)c);
+    if (ext == "sf2" || ext == "sf3" || ext == "sfbk") return kh_bank_open_sf2(path, cfg, opt);
+    if (ext == "sfz") return kh_bank_open_sfz(path, cfg, opt);
+    g_err = p + ": unrecognised soundfont extension \"" + ext + "\"; expected .sf2 or .sfz";
+    return nullptr;
+}
+
+const char* kh_bank_report(const kh_bank* b) { return b ? b->report.c_str() : ""; }
+
+int kh_sfz_note_name(const char* s, int32_t* out) { return s && out && sfz_note_name(s, out) ? 0 : 1; }
+size_t kh_sfz_value_end(const char* s) { return s ? sfz_value_end(s) : 0; }
 
 int kh_sf2_write_synthetic(const kh_synth_bank_spec* spec, const char* path) {
     if (!spec || !path) {

@@ -78,6 +78,11 @@ HOST_SYMBOLS = {
     "kh_bank_synthetic": (_P, [C.POINTER(KhSynthBankSpec), C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
     "kh_bank_destroy": (None, [_P]),
     "kh_bank_open_sf2": (_P, [C.c_char_p, C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
+    "kh_bank_open_sfz": (_P, [C.c_char_p, C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
+    "kh_bank_open": (_P, [C.c_char_p, C.POINTER(N.KcConfig), C.POINTER(KhOptions)]),
+    "kh_bank_report": (C.c_char_p, [_P]),
+    "kh_sfz_note_name": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),
+    "kh_sfz_value_end": (C.c_size_t, [C.c_char_p]),
     "kh_sf2_write_synthetic": (C.c_int, [C.POINTER(KhSynthBankSpec), C.c_char_p]),
     "kh_bank_samples": (C.c_uint32, [_P]),
     "kh_bank_region_info": (C.c_int, [_P, C.c_uint32, C.POINTER(KhRegionInfo)]),
@@ -383,7 +388,7 @@ def midi_spec(**kw) -> KhMidiSpec:
 
 class Bank:
     """A loaded bank: the i16 sample pool and the variant-0 params table.
-    `spec` is a synthetic bank spec or the path of a SoundFont 2 file."""
+    `spec` is a synthetic bank spec or the path of a soundfont (.sf2 or .sfz)."""
 
     def __init__(self, spec, cfg: N.KcConfig, opt: KhOptions | None = None):
         self._lib = lib()
@@ -391,7 +396,7 @@ class Bank:
         if isinstance(spec, KhSynthBankSpec):
             h = self._lib.kh_bank_synthetic(C.byref(spec), C.byref(cfg), C.byref(self.opt))
         else:
-            h = self._lib.kh_bank_open_sf2(str(spec).encode(), C.byref(cfg), C.byref(self.opt))
+            h = self._lib.kh_bank_open(str(spec).encode(), C.byref(cfg), C.byref(self.opt))
         if not h:
             raise RuntimeError(self._lib.kh_last_error().decode())
         self._h = h
@@ -408,6 +413,11 @@ class Bank:
         self.presets = self._lib.kh_bank_presets(h)
         self.max_sample_len = self._lib.kh_bank_max_sample_len(h)
         self.pool_rate = self._lib.kh_bank_pool_rate(h)
+
+    @property
+    def report(self) -> list[str]:
+        """The loader's warnings (unreadable samples, unsupported opcodes)."""
+        return [x for x in self._lib.kh_bank_report(self._h).decode().split("\n") if x]
 
     @property
     def n_samples(self) -> int:
