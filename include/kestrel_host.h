@@ -12,6 +12,7 @@
  *                   admission preview tables, params variants
  *   src/sf2.rs      the RIFF walk, preset/instrument flattening
  *                   (build_region) and build_pool
+ *   src/sfz.rs      SFZ instruments, with the WAV reader of src/wav.rs
  *   src/resample.rs the load-time 32-tap x 512-phase Blackman sinc
  *   src/voice.rs    GateTable, ChannelTable, admit_key/mix48/rank_gain_q
  *   src/midi.rs     MidiStream (standard MIDI files) and TempoClock
@@ -21,8 +22,8 @@
  *                   from, and the SF2 writer's layout
  *   src/limiter.rs, src/wav.rs  the output stage
  *
- * A soundfont is a SoundFont 2 file or a seeded synthetic bank (written in
- * the same format and loaded by the same code); MIDI is a standard MIDI file
+ * A soundfont is a SoundFont 2 file, an SFZ instrument, or a seeded synthetic
+ * bank (written as SF2 and loaded by the same code); MIDI is a standard MIDI file
  * or a seeded synthetic event stream with the shapes of the benchmark
  * configurations. The block inputs it produces are the backend's arguments
  * verbatim: kc_spawn_cmd records, gate rows, channel rows.
