@@ -228,6 +228,9 @@ typedef struct kh_block {
     uint32_t take;                /* candidates admitted */
     uint64_t block_index;
     uint64_t notes;               /* note-ons handled so far */
+    uint64_t want_energy;         /* summed opening amplitude (15-bit rank gains) of the
+                                     queued layers, and of the admitted ones */
+    uint64_t take_energy;         /* (DriverStats::last_want/take_energy, src/driver.rs:178-182) */
 } kh_block;
 
 kh_driver* kh_driver_open(const kc_config* cfg, const kh_options* opt, const kh_bank* bank,

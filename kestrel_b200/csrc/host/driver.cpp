@@ -98,6 +98,7 @@ struct Driver {
     std::vector<std::pair<uint32_t, std::vector<kc_region_params>>> built;
     uint64_t notes_total = 0;
     uint32_t last_want = 0, last_take = 0, last_live = 0;
+    uint64_t last_want_energy = 0, last_take_energy = 0;
     bool done_after_admit = false;
 
     // Driver::open, src/driver.rs:343-413.
@@ -283,6 +284,14 @@ struct Driver {
             } else {
                 rank_candidates(want, take);
             }
+        }
+        // Summed opening amplitude of the queued and of the admitted layers,
+        // after the rule has reordered (src/driver.rs:581-585).
+        last_want_energy = last_take_energy = 0;
+        for (size_t i = 0; i < cands.size(); ++i) {
+            const uint64_t e = (cands[i].key >> 48) & 0x7FFF;
+            last_want_energy += e;
+            if (i < take) last_take_energy += e;
         }
         materialise(take);
         // What finish() decides the next block by, as of this block.
@@ -1000,6 +1009,8 @@ int kh_driver_prepare(kh_driver* h, uint32_t live, kh_block* out) {
     out->take = d.last_take;
     out->block_index = d.block_index;
     out->notes = d.notes_total;
+    out->want_energy = d.last_want_energy;
+    out->take_energy = d.last_take_energy;
     return 0;
 }
 
@@ -1038,6 +1049,8 @@ int kh_driver_admit(kh_driver* h, uint32_t live, kh_block* out) {
     out->take = d.last_take;
     out->block_index = d.block_index;
     out->notes = d.notes_total;
+    out->want_energy = d.last_want_energy;
+    out->take_energy = d.last_take_energy;
     return 0;
 }
 

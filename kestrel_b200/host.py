@@ -46,7 +46,8 @@ class KhBlock(C.Structure):
     _fields_ = [("gates", C.POINTER(C.c_uint32)), ("n_gates", C.c_size_t), ("chan", C.POINTER(C.c_uint32)),
                 ("n_chan", C.c_size_t), ("bend", C.c_int), ("gain", C.c_int), ("variant", C.c_int),
                 ("cmds", C.c_void_p), ("n_cmds", C.c_size_t), ("n_variants", C.c_uint32), ("live", C.c_uint32),
-                ("want", C.c_uint32), ("take", C.c_uint32), ("block_index", C.c_uint64), ("notes", C.c_uint64)]
+                ("want", C.c_uint32), ("take", C.c_uint32), ("block_index", C.c_uint64), ("notes", C.c_uint64),
+                ("want_energy", C.c_uint64), ("take_energy", C.c_uint64)]
 
 
 class KhRegionInfo(C.Structure):
@@ -476,6 +477,8 @@ class BlockInputs:
     live: int = 0
     want: int = 0
     take: int = 0
+    want_energy: int = 0
+    take_energy: int = 0
 
 
 class Driver:
@@ -559,7 +562,7 @@ class Driver:
             arr = np.frombuffer((C.c_char * (n.value * 48)).from_address(data.value), dtype=N.PARAMS_DTYPE).copy()
             variants.append((idx.value, arr))
         return BlockInputs(gates, chan, bool(b.bend), bool(b.gain), bool(b.variant), cmds, variants, b.live, b.want,
-                           b.take)
+                           b.take, b.want_energy, b.take_energy)
 
     def finish(self, active_voices: int) -> bool:
         more = C.c_int()

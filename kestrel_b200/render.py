@@ -55,14 +55,41 @@ def cuda_backend(cfg, bank: H.Bank):
     return CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)
 
 
+class BlockCsv:
+    """`--block-csv` (src/bin/kestrel.rs:301-340): one row per block with the
+    admission decision and the level it produced."""
+
+    HEADER = "block,t,live,want,take,stolen,dropped,rms,peak,want_e,take_e\n"
+
+    def __init__(self, path, sample_rate: int):
+        self.f = open(path, "w")
+        self.f.write(self.HEADER)
+        self.rate = sample_rate
+        self.dropped = 0
+
+    def row(self, block: int, frames: int, adm, stolen: int, out: np.ndarray) -> None:
+        """adm: (live, want, take, want_energy, take_energy) of the block."""
+        live, want, take, we, te = adm
+        self.dropped += want - take
+        x = out.astype(np.float64)
+        rms = float(np.sqrt(np.dot(x, x) / max(out.size, 1)))
+        peak = float(np.max(np.abs(out))) if out.size else 0.0
+        self.f.write(f"{block},{frames / self.rate:.6f},{live},{want},{take},{stolen},{self.dropped},"
+                     f"{rms:.9f},{peak:.9f},{we},{te}\n")
+
+    def close(self) -> None:
+        self.f.close()
+
+
 def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: int = H.LIMITER_BRICKWALL,
                 fmt: int = H.WAV_FLOAT32, max_seconds: float = 0.0, limiter_opts: dict | None = None,
-                on_block=None, pipelined: bool | None = None, options=None) -> RenderStats:
+                on_block=None, pipelined: bool | None = None, options=None, block_csv=None) -> RenderStats:
     """Render (cfg, soundfont spec, MIDI spec or MIDI file path) into `path`
     until the stream ends or `max_seconds` of audio (0: no bound).
     `backend(cfg, bank)` makes the Backend (the CUDA one by default).
     `pipelined` (default: whenever the backend can) overlaps the host's work
-    with the backend's render. `options` are the driver's kh_options."""
+    with the backend's render. `options` are the driver's kh_options;
+    `block_csv` a path for the per-block diagnostic rows."""
     bank = H.Bank(bank_spec, cfg, options)
     drv = H.Driver(cfg, bank, midi_spec)
     synth = backend(cfg, bank)
@@ -71,13 +98,16 @@ def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: 
     max_frames = int(max_seconds * cfg.sample_rate) if max_seconds > 0 else 0
     if pipelined is None:
         pipelined = hasattr(synth, "render_begin")
+    csv = BlockCsv(block_csv, cfg.sample_rate) if block_csv else None
     t0 = time.perf_counter()
     try:
         if pipelined:
-            blocks, frames, peak_voices, phases = _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block)
+            blocks, frames, peak_voices, phases = _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block, csv)
         else:
-            blocks, frames, peak_voices, phases = _serial(drv, synth, lim, wav, cfg, max_frames, on_block)
+            blocks, frames, peak_voices, phases = _serial(drv, synth, lim, wav, cfg, max_frames, on_block, csv)
     finally:
+        if csv:
+            csv.close()
         data_bytes = wav.finish()
         wall = time.perf_counter() - t0
         synth.close()
@@ -86,11 +116,12 @@ def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: 
                        pipelined, phases)
 
 
-def _serial(drv, synth, lim, wav, cfg, max_frames, on_block):
+def _serial(drv, synth, lim, wav, cfg, max_frames, on_block, csv=None):
     """The reference's loop as written: prepare, feed, render, output, finish."""
     frames = blocks = peak_voices = 0
     while True:
-        blk = drv.prepare(synth.stats().active_voices)
+        st0 = synth.stats()
+        blk = drv.prepare(st0.active_voices)
         H.feed(synth, blk)
         out = synth.render()
         lim.process(out)
@@ -101,13 +132,16 @@ def _serial(drv, synth, lim, wav, cfg, max_frames, on_block):
         peak_voices = max(peak_voices, st.active_voices)
         frames += cfg.block_frames
         blocks += 1
+        if csv:
+            csv.row(blocks, frames, (blk.live, blk.want, blk.take, blk.want_energy, blk.take_energy),
+                    st.stolen - st0.stolen, out)
         more = drv.finish(st.active_voices)
         if not more or (max_frames and frames >= max_frames):
             break
     return blocks, frames, peak_voices, None
 
 
-def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block):
+def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block, csv=None):
     """The same calls as _serial, reordered so the host overlaps the device:
     collect(n + 1) runs while block n renders, and block n's limiter and WAV
     write run while block n + 1 renders."""
@@ -116,9 +150,12 @@ def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block):
     frames = blocks = peak_voices = 0
     bufs = [np.empty(cfg.block_frames * 2, np.float32) for _ in range(2)]
 
+    adm = []   # admission of the blocks in flight, for the diagnostic rows
+
     def launch(live):
         t = clock()
         kb = drv.admit_raw(live)
+        adm.append((kb.live, kb.want, kb.take, kb.want_energy, kb.take_energy))
         synth.feed_raw(kb, drv.variant_ptrs(kb))
         synth.render_begin()
         drv.advance()
@@ -127,6 +164,7 @@ def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block):
     t = clock()
     drv.collect()
     ph["collect"] += clock() - t
+    stolen = synth.stats().stolen
     launch(synth.stats().active_voices)
     while True:
         t = clock()
@@ -151,6 +189,9 @@ def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block):
         ph["output"] += clock() - t
         if on_block:
             on_block(n, out)
+        if csv:
+            csv.row(blocks, frames, adm.pop(0), st.stolen - stolen, out)
+        stolen = st.stolen
         if stop:
             return blocks, frames, peak_voices, ph
 
@@ -211,6 +252,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-resample-pool", action="store_true")
     ap.add_argument("--pool-budget", type=int, default=2048, help="sample pool budget in MiB")
     ap.add_argument("--seconds", type=float, default=0.0, help="stop after this much audio (0: the whole file)")
+    ap.add_argument("--block-csv", default=None, metavar="PATH",
+                    help="one row per block: the admission decision and the level it produced")
     ap.add_argument("--serial", action="store_true", help="the reference's serial loop instead of the pipelined one")
     ap.add_argument("--no-read-ahead", action="store_true", help="read MIDI events on the driver's thread")
     args = ap.parse_args(argv)
@@ -249,7 +292,8 @@ def main(argv=None) -> int:
     lim_opts = dict(ceiling_db=args.ceiling_db, lookahead_ms=args.lookahead_ms, release_ms=args.limiter_release_ms,
                     sustain_ms=args.limiter_sustain_ms, true_peak=not args.no_true_peak)
     st = render_file(args.out, cfg, bs, ms, limiter=mode, fmt=fmt, max_seconds=args.seconds,
-                     pipelined=False if args.serial else None, options=opt, limiter_opts=lim_opts)
+                     pipelined=False if args.serial else None, options=opt, limiter_opts=lim_opts,
+                     block_csv=args.block_csv)
     print(f"{st.seconds:.2f} s rendered in {st.wall_s:.2f} s ({st.x_realtime:.2f}x realtime), {st.blocks} blocks, "
           f"peak {st.peak_voices} voices, {st.clipped} samples clipped, {st.data_bytes} bytes"
           + (", host s: " + ", ".join(f"{k} {v:.2f}" for k, v in st.phases.items()) if st.phases else ""),

@@ -266,3 +266,25 @@ def test_read_ahead_leaves_the_blocks_unchanged(tmp_path, workload, over):
         assert a.finish(live) == b.finish(live)
     a.close()
     b.close()
+
+
+def test_block_csv_rows_match_between_the_loops(tmp_path):
+    """`--block-csv`: the same rows from the serial and the pipelined loop;
+    admission never takes more than it queued, the drop count accumulates
+    want - take, and the energies bound each other."""
+    import csv as pycsv
+    cfg, bs, ms = _spec("black", notes=30000, seconds=0.5, cluster_lo=500, cluster_hi=3000, max_voices=2048,
+                        admit_rule=N.ADMIT_LOUDEST)
+    render_file(tmp_path / "a.wav", cfg, bs, ms, backend=_oracle, block_csv=tmp_path / "a.csv")
+    render_file(tmp_path / "b.wav", cfg, bs, ms, backend=_tracking_async, block_csv=tmp_path / "b.csv")
+    assert (tmp_path / "a.csv").read_text() == (tmp_path / "b.csv").read_text()
+    rows = list(pycsv.DictReader(open(tmp_path / "a.csv")))
+    assert [int(r["block"]) for r in rows] == list(range(1, len(rows) + 1))
+    dropped = 0
+    for r in rows:
+        want, take = int(r["want"]), int(r["take"])
+        assert take <= want and int(r["take_e"]) <= int(r["want_e"])
+        dropped += want - take
+        assert int(r["dropped"]) == dropped
+        assert 0.0 <= float(r["rms"]) <= float(r["peak"]) <= 1.0
+    assert dropped > 0 and any(int(r["stolen"]) > 0 for r in rows)

@@ -67,9 +67,9 @@ def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
     from kestrel_b200 import render as R
     seen = {}
 
-    def fake(path, cfg, bank, midi, limiter, fmt, max_seconds, pipelined, options, limiter_opts):
+    def fake(path, cfg, bank, midi, limiter, fmt, max_seconds, pipelined, options, limiter_opts, block_csv):
         seen.update(path=path, cfg=cfg, bank=bank, midi=midi, limiter=limiter, fmt=fmt, seconds=max_seconds,
-                    pipelined=pipelined, opt=options, lim=limiter_opts)
+                    pipelined=pipelined, opt=options, lim=limiter_opts, csv=block_csv)
         return R.RenderStats(1, 0.1, 0.1, 0, 0, 0, 0)
 
     monkeypatch.setattr(R, "render_file", fake)
@@ -77,7 +77,7 @@ def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
             "--max-voices", "5000", "--interp", "hermite", "--decay-curve", "lin", "--steal", "drop-new",
             "--admit", "spread", "--steal-percent", "50", "--format", "pcm16", "--volume", "0.5", "--layers", "4",
             "--ceiling-db", "-1", "--no-true-peak", "--no-filter", "--no-sort", "--no-resample-pool",
-            "--pool-budget", "64", "--seconds", "3", "--serial"])
+            "--pool-budget", "64", "--seconds", "3", "--serial", "--block-csv", "b.csv"])
     c, o = seen["cfg"], seen["opt"]
     assert seen["midi"] == "song.mid" and seen["bank"] == "bank.sf2"
     assert (c.sample_rate, c.block_frames, c.max_voices, c.max_steal_percent) == (44100, 2048, 5000, 50)
@@ -86,7 +86,7 @@ def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
     assert (o.filter_enabled, o.resample_pool, o.sample_pool_budget, o.max_layers) == (0, 0, 64 << 20, 4)
     assert abs(o.master_volume - 0.5) < 1e-7
     assert seen["fmt"] == H.WAV_PCM16 and seen["seconds"] == 3.0 and seen["pipelined"] is False
-    assert seen["lim"]["ceiling_db"] == -1.0 and seen["lim"]["true_peak"] is False
+    assert seen["lim"]["ceiling_db"] == -1.0 and seen["lim"]["true_peak"] is False and seen["csv"] == "b.csv"
     R.main(["-o", str(tmp_path / "o.wav"), "--no-limiter"])
     assert seen["limiter"] == H.LIMITER_OFF and seen["pipelined"] is None
     with pytest.raises(SystemExit):
