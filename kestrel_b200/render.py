@@ -83,13 +83,16 @@ class BlockCsv:
 
 def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: int = H.LIMITER_BRICKWALL,
                 fmt: int = H.WAV_FLOAT32, max_seconds: float = 0.0, limiter_opts: dict | None = None,
-                on_block=None, pipelined: bool | None = None, options=None, block_csv=None) -> RenderStats:
+                on_block=None, pipelined: bool | None = None, options=None, block_csv=None,
+                nan_guard: bool = False, progress=None) -> RenderStats:
     """Render (cfg, soundfont spec, MIDI spec or MIDI file path) into `path`
     until the stream ends or `max_seconds` of audio (0: no bound).
     `backend(cfg, bank)` makes the Backend (the CUDA one by default).
     `pipelined` (default: whenever the backend can) overlaps the host's work
     with the backend's render. `options` are the driver's kh_options;
-    `block_csv` a path for the per-block diagnostic rows."""
+    `block_csv` a path for the per-block diagnostic rows; `nan_guard` stops
+    at the first block holding a NaN or an infinity; `progress(seconds,
+    voices, x_realtime, timings)` is called about once a second."""
     bank = H.Bank(bank_spec, cfg, options)
     drv = H.Driver(cfg, bank, midi_spec)
     synth = backend(cfg, bank)
@@ -100,6 +103,19 @@ def render_file(path, cfg, bank_spec, midi_spec, backend=cuda_backend, limiter: 
         pipelined = hasattr(synth, "render_begin")
     csv = BlockCsv(block_csv, cfg.sample_rate) if block_csv else None
     t0 = time.perf_counter()
+    if nan_guard or progress:
+        user_cb, last = on_block, [t0]
+
+        def on_block(n, out):
+            if nan_guard and not np.isfinite(out).all():
+                raise FloatingPointError(f"block {n}: non-finite samples in the output")
+            if progress and time.perf_counter() - last[0] > 1.0:
+                last[0] = time.perf_counter()
+                secs = (n + 1) * cfg.block_frames / cfg.sample_rate
+                t = synth.timings() if hasattr(synth, "timings") else []
+                progress(secs, synth.stats().active_voices, secs / max(last[0] - t0, 1e-9), t)
+            if user_cb:
+                user_cb(n, out)
     try:
         if pipelined:
             blocks, frames, peak_voices, phases = _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block, csv)
@@ -252,6 +268,9 @@ def main(argv=None) -> int:
     ap.add_argument("--no-resample-pool", action="store_true")
     ap.add_argument("--pool-budget", type=int, default=2048, help="sample pool budget in MiB")
     ap.add_argument("--seconds", type=float, default=0.0, help="stop after this much audio (0: the whole file)")
+    ap.add_argument("--profile", action="store_true", help="log per-pass device timings with the progress line")
+    ap.add_argument("--nan-guard", action="store_true", help="stop at the first block with a NaN or an infinity")
+    ap.add_argument("--quiet", action="store_true", help="no progress lines")
     ap.add_argument("--block-csv", default=None, metavar="PATH",
                     help="one row per block: the admission decision and the level it produced")
     ap.add_argument("--serial", action="store_true", help="the reference's serial loop instead of the pipelined one")
@@ -291,9 +310,20 @@ def main(argv=None) -> int:
     fmt = H.WAV_FLOAT32 if args.format == "float32" else H.WAV_PCM16
     lim_opts = dict(ceiling_db=args.ceiling_db, lookahead_ms=args.lookahead_ms, release_ms=args.limiter_release_ms,
                     sustain_ms=args.limiter_sustain_ms, true_peak=not args.no_true_peak)
-    st = render_file(args.out, cfg, bs, ms, limiter=mode, fmt=fmt, max_seconds=args.seconds,
+    def progress(secs, voices, xrt, timings):
+        print(f"{secs:8.2f}s rendered | {voices:10d} voices | {xrt:.2f}x realtime", file=sys.stderr, flush=True)
+        if args.profile and timings:
+            print("  passes: " + "  ".join(f"{n} {ms:.3f}ms" for n, ms in timings), file=sys.stderr, flush=True)
+
+    def backend(cfg, bank):
+        s = cuda_backend(cfg, bank)
+        if args.profile:
+            s.set_profile(True)
+        return s
+
+    st = render_file(args.out, cfg, bs, ms, backend=backend, limiter=mode, fmt=fmt, max_seconds=args.seconds,
                      pipelined=False if args.serial else None, options=opt, limiter_opts=lim_opts,
-                     block_csv=args.block_csv)
+                     block_csv=args.block_csv, nan_guard=args.nan_guard, progress=None if args.quiet else progress)
     print(f"{st.seconds:.2f} s rendered in {st.wall_s:.2f} s ({st.x_realtime:.2f}x realtime), {st.blocks} blocks, "
           f"peak {st.peak_voices} voices, {st.clipped} samples clipped, {st.data_bytes} bytes"
           + (", host s: " + ", ".join(f"{k} {v:.2f}" for k, v in st.phases.items()) if st.phases else ""),

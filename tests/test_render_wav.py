@@ -67,9 +67,10 @@ def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
     from kestrel_b200 import render as R
     seen = {}
 
-    def fake(path, cfg, bank, midi, limiter, fmt, max_seconds, pipelined, options, limiter_opts, block_csv):
+    def fake(path, cfg, bank, midi, backend, limiter, fmt, max_seconds, pipelined, options, limiter_opts, block_csv,
+             nan_guard, progress):
         seen.update(path=path, cfg=cfg, bank=bank, midi=midi, limiter=limiter, fmt=fmt, seconds=max_seconds,
-                    pipelined=pipelined, opt=options, lim=limiter_opts, csv=block_csv)
+                    pipelined=pipelined, opt=options, lim=limiter_opts, csv=block_csv, nan=nan_guard, prog=progress)
         return R.RenderStats(1, 0.1, 0.1, 0, 0, 0, 0)
 
     monkeypatch.setattr(R, "render_file", fake)
@@ -77,7 +78,7 @@ def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
             "--max-voices", "5000", "--interp", "hermite", "--decay-curve", "lin", "--steal", "drop-new",
             "--admit", "spread", "--steal-percent", "50", "--format", "pcm16", "--volume", "0.5", "--layers", "4",
             "--ceiling-db", "-1", "--no-true-peak", "--no-filter", "--no-sort", "--no-resample-pool",
-            "--pool-budget", "64", "--seconds", "3", "--serial", "--block-csv", "b.csv"])
+            "--pool-budget", "64", "--seconds", "3", "--serial", "--block-csv", "b.csv", "--nan-guard", "--quiet"])
     c, o = seen["cfg"], seen["opt"]
     assert seen["midi"] == "song.mid" and seen["bank"] == "bank.sf2"
     assert (c.sample_rate, c.block_frames, c.max_voices, c.max_steal_percent) == (44100, 2048, 5000, 50)
@@ -87,7 +88,32 @@ def test_cli_maps_the_reference_render_flags(tmp_path, monkeypatch):
     assert abs(o.master_volume - 0.5) < 1e-7
     assert seen["fmt"] == H.WAV_PCM16 and seen["seconds"] == 3.0 and seen["pipelined"] is False
     assert seen["lim"]["ceiling_db"] == -1.0 and seen["lim"]["true_peak"] is False and seen["csv"] == "b.csv"
+    assert seen["nan"] is True and seen["prog"] is None
     R.main(["-o", str(tmp_path / "o.wav"), "--no-limiter"])
     assert seen["limiter"] == H.LIMITER_OFF and seen["pipelined"] is None
     with pytest.raises(SystemExit):
         R.main(["x.mid", "-o", "y.wav", "--steal", "loudest"])
+
+
+def test_nan_guard_stops_at_a_non_finite_block(tmp_path):
+    """--nan-guard: a block holding a NaN ends the render with an error (the
+    NaN is planted in the CPU reference's output)."""
+    class Planted:
+        def __init__(self, cfg, bank):
+            self.o, self.n = _oracle(cfg, bank), 0
+            self.block_frames = cfg.block_frames
+
+        def __getattr__(self, name):
+            return getattr(self.o, name)
+
+        def render(self):
+            out = self.o.render()
+            self.n += 1
+            if self.n == 3:
+                out[5] = np.nan
+            return out
+
+    cfg, bs, ms = H.config_workload("plain", seed=2)
+    render_file(tmp_path / "ok.wav", cfg, bs, ms, backend=Planted, max_seconds=0.3)   # unguarded: runs on
+    with pytest.raises(FloatingPointError, match="block 2"):
+        render_file(tmp_path / "x.wav", cfg, bs, ms, backend=Planted, max_seconds=0.3, nan_guard=True)
