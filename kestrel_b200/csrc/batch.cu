@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(256) kb_spawn(const BatchHeader* hdr, const Jo
 
 // ---- render, fold ----------------------------------------------------------------
 
-template <int INTERP, bool STRICT, int MIX, int V>
+template <int INTERP, bool STRICT, int MIX, int V, bool DOUBLE = false>
 __global__ void __launch_bounds__(RENDER_WARPS * 32, V == 1 ? 3 : 2)
 kb_render(const BatchHeader* hdr, const JobDesc* jobs, BatchPlan* plan) {
     extern __shared__ float4 smem4[];
@@ -254,8 +254,8 @@ kb_render(const BatchHeader* hdr, const JobDesc* jobs, BatchPlan* plan) {
         __syncwarp();
         const uint32_t tw = d.pa.render_warps;
         const uint32_t nv = a.st->live_render;
-        if (a.ctl->chan_active) render_batches<INTERP, true, STRICT, MIX, V>(a, sm, k, tw, nv);
-        else render_batches<INTERP, false, STRICT, MIX, V>(a, sm, k, tw, nv);
+        if (a.ctl->chan_active) render_batches<INTERP, true, STRICT, MIX, V, true, DOUBLE>(a, sm, k, tw, nv);
+        else render_batches<INTERP, false, STRICT, MIX, V, true, DOUBLE>(a, sm, k, tw, nv);
         __syncwarp();
     }
 }
@@ -367,33 +367,37 @@ __global__ void __launch_bounds__(256) kb_collect(const BatchHeader* hdr, const 
     }
 }
 
-template <int I, bool S, int M, int V>
+template <int I, bool S, int M, int V, bool D = false>
 void* render_fn() {
-    return reinterpret_cast<void*>(&kb_render<I, S, M, V>);
+    return reinterpret_cast<void*>(&kb_render<I, S, M, V, D>);
 }
 
+// The 32-frame unit tiles (`dbl`) exist for the linear interpolator, the
+// f32 mix and one voice per lane; null elsewhere.
 template <int I, bool S, int M>
-void* render_v(uint32_t v) {
-    if constexpr (I == KC_INTERP_LINEAR && M == KC_MIX_F32_TREE)
-        if (v == 2) return render_fn<I, S, M, 2>();
-    return render_fn<I, S, M, 1>();
+void* render_v(uint32_t v, bool dbl) {
+    if constexpr (I == KC_INTERP_LINEAR && M == KC_MIX_F32_TREE) {
+        if (v == 2) return dbl ? nullptr : render_fn<I, S, M, 2>();
+        if (dbl) return render_fn<I, S, M, 1, true>();
+    }
+    return dbl ? nullptr : render_fn<I, S, M, 1>();
 }
 
 template <int I, bool S>
-void* render_m(uint32_t mix, uint32_t v) {
-    if (mix == KC_MIX_TWO_SUM) return render_v<I, S, KC_MIX_TWO_SUM>(v);
-    if (mix == KC_MIX_F64) return render_v<I, S, KC_MIX_F64>(v);
-    return render_v<I, S, KC_MIX_F32_TREE>(v);
+void* render_m(uint32_t mix, uint32_t v, bool dbl) {
+    if (mix == KC_MIX_TWO_SUM) return render_v<I, S, KC_MIX_TWO_SUM>(v, dbl);
+    if (mix == KC_MIX_F64) return render_v<I, S, KC_MIX_F64>(v, dbl);
+    return render_v<I, S, KC_MIX_F32_TREE>(v, dbl);
 }
 
-void* batch_render_fn(uint32_t interp, bool strict, uint32_t mix, uint32_t v) {
+void* batch_render_fn(uint32_t interp, bool strict, uint32_t mix, uint32_t v, bool dbl = false) {
     switch (interp) {
         case KC_INTERP_NEAREST:
-            return strict ? render_m<0, true>(mix, v) : render_m<0, false>(mix, v);
+            return strict ? render_m<0, true>(mix, v, dbl) : render_m<0, false>(mix, v, dbl);
         case KC_INTERP_LINEAR:
-            return strict ? render_m<1, true>(mix, v) : render_m<1, false>(mix, v);
+            return strict ? render_m<1, true>(mix, v, dbl) : render_m<1, false>(mix, v, dbl);
         default:
-            return strict ? render_m<2, true>(mix, v) : render_m<2, false>(mix, v);
+            return strict ? render_m<2, true>(mix, v, dbl) : render_m<2, false>(mix, v, dbl);
     }
 }
 
@@ -413,6 +417,8 @@ struct kc_batch {
     uint32_t vpl = 1;
     uint32_t radix = 8;
     void* render_fn = nullptr;
+    void* render_fn2 = nullptr;    // 32-frame unit tiles (null where not built)
+    bool unit_tiles = false;       // the last batch ran mostly on unit spans
     size_t render_smem = 0;
     uint32_t render_ctas = 0;
     uint32_t pass_ctas = 0;
@@ -427,8 +433,8 @@ struct kc_batch {
     char* h_stage = nullptr;       // pinned readback
     size_t job_stride = 0;         // bytes per job in the stage
 
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr, graph2 = nullptr;
+    cudaGraphExec_t exec = nullptr, exec2 = nullptr;  // 16- and 32-frame unit tiles
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.0f;
     uint64_t blocks = 0;
@@ -449,6 +455,8 @@ void free_batch(kc_batch* b) {
     if (!b) return;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->exec2) cudaGraphExecDestroy(b->exec2);
+    if (b->graph2) cudaGraphDestroy(b->graph2);
     cudaFree(b->d_hdr);
     cudaFree(b->d_plan);
     cudaFree(b->d_stage);
@@ -462,7 +470,7 @@ void free_batch(kc_batch* b) {
 // The block's launches, in the single-context order. Every launch reads the
 // job count and its items from device memory, so the sequence is the same for
 // every block and every job set.
-int enqueue_passes(kc_batch* b) {
+int enqueue_passes(kc_batch* b, void* render_fn) {
     cudaStream_t q = b->stream;
     const uint32_t P = b->pass_ctas;
     const BatchHeader* h = b->d_hdr;
@@ -477,7 +485,7 @@ int enqueue_passes(kc_batch* b) {
     kb_mark<<<P, 256, 0, q>>>(h, J, pl);
     kb_spawn<<<P, 256, 0, q>>>(h, J, pl);
     void* args[] = {(void*)&h, (void*)&J, (void*)&pl};
-    KB_CUDA(cudaLaunchKernel(b->render_fn, dim3(b->render_ctas), dim3(RENDER_WARPS * 32), args, b->render_smem, q));
+    KB_CUDA(cudaLaunchKernel(render_fn, dim3(b->render_ctas), dim3(RENDER_WARPS * 32), args, b->render_smem, q));
     if (b->cfg.mix_mode == KC_MIX_F32_TREE) kb_reduce<KC_MIX_F32_TREE><<<P, 256, 0, q>>>(h, J, pl);
     else if (b->cfg.mix_mode == KC_MIX_TWO_SUM) kb_reduce<KC_MIX_TWO_SUM><<<P, 256, 0, q>>>(h, J, pl);
     else kb_reduce<KC_MIX_F64><<<P, 256, 0, q>>>(h, J, pl);
@@ -555,6 +563,10 @@ int kc_batch_create(const kc_batch_config* cfg, kc_batch** out) {
     KB_TRY(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
     KB_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     b->render_fn = batch_render_fn(cfg->interpolation, cfg->strict_fp != 0, cfg->mix_mode, b->vpl);
+    b->render_fn2 = batch_render_fn(cfg->interpolation, cfg->strict_fp != 0, cfg->mix_mode, b->vpl, true);
+    if (b->render_fn2)
+        KB_TRY(cudaFuncSetAttribute(b->render_fn2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)((size_t)RENDER_WARPS * SM_WARP * sizeof(float))));
     b->render_smem = (size_t)RENDER_WARPS * SM_WARP * sizeof(float);
     KB_TRY(cudaFuncSetAttribute(b->render_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->render_smem));
     int per_sm = 0;
@@ -576,17 +588,21 @@ int kc_batch_create(const kc_batch_config* cfg, kc_batch** out) {
     KB_TRY(cudaEventCreate(&b->ev0));
     KB_TRY(cudaEventCreate(&b->ev1));
     if (cfg->use_graph) {
-        KB_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        const int rc = enqueue_passes(b);
-        cudaGraph_t g = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
-        if (rc) {
-            if (g) cudaGraphDestroy(g);
-            return bail(rc);
+        for (int k = 0; k < 2; ++k) {
+            void* fn = k ? b->render_fn2 : b->render_fn;
+            if (!fn) continue;
+            KB_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue_passes(b, fn);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return bail(rc);
+            }
+            KB_TRY(e);
+            (k ? b->graph2 : b->graph) = g;
+            KB_TRY(cudaGraphInstantiate(k ? &b->exec2 : &b->exec, g, 0));
         }
-        KB_TRY(e);
-        b->graph = g;
-        KB_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
     }
     KB_TRY(cudaStreamSynchronize(b->stream));
 #undef KB_TRY
@@ -707,14 +723,18 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
     const size_t table = sizeof(BatchHeader) + (size_t)n_jobs * sizeof(JobDesc);
     KB_CUDA(cudaMemcpyAsync(b->d_hdr, b->h_table, table, cudaMemcpyHostToDevice, q));
     KB_CUDA(cudaEventRecord(b->ev0, q));
-    if (b->exec) KB_CUDA(cudaGraphLaunch(b->exec, q));
-    else if (int rc = enqueue_passes(b)) return rc;
+    // Both tile lengths leave the same bits; the last batch's unit-path
+    // share picks the faster one.
+    const bool dbl = b->unit_tiles && b->render_fn2;
+    if (b->exec && (!dbl || b->exec2)) KB_CUDA(cudaGraphLaunch(dbl ? b->exec2 : b->exec, q));
+    else if (int rc = enqueue_passes(b, dbl ? b->render_fn2 : b->render_fn)) return rc;
     KB_CUDA(cudaEventRecord(b->ev1, q));
     if (n_jobs) KB_CUDA(cudaMemcpyAsync(b->h_stage, b->d_stage, b->job_stride * n_jobs, cudaMemcpyDeviceToHost, q));
     KB_CUDA(cudaStreamSynchronize(q));
     cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
     b->blocks += 1;
     int rc = KC_OK;
+    uint64_t unit = 0, all = 0;
     for (uint32_t j = 0; j < n_jobs; ++j) {
         kc_synth* s = jobs[j];
         const char* row = b->h_stage + b->job_stride * j;
@@ -729,9 +749,13 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         s->stats.stolen = st.stolen;
         s->stats.dropped = st.dropped;
         std::memcpy(&s->stats.peak, &st.peak_bits, 4);
+        unit += st.unit_tiles;
+        all += st.all_tiles;
+        if (st.all_tiles) s->unit_tiles = (uint64_t)st.unit_tiles * 2u >= st.all_tiles;
         if (st.error && rc == KC_OK)
             rc = fail(KC_ERR_DEVICE, "job " + std::to_string(j) + ": device error word " + std::to_string(st.error));
     }
+    if (all) b->unit_tiles = unit * 2u >= all;
     return rc;
 }
 

@@ -108,6 +108,19 @@ def test_batch_matches_alone_other_mixes(mix_mode):
 
 
 @gpu
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_matches_alone_on_unit_spans(use_graph):
+    """Unit and integral-step jobs: from the second batch on the batch runs
+    its 32-frame unit-tile graph, and every job still matches itself alone."""
+    scs = [make_scenario(seed=31 + i, max_voices=20000, n_blocks=6, spawn_per_block=(3000, 6000), release_rate=0.03,
+                         sort_voices=1, steps=st, chan=ch, bend_prob=0.02, block_frames=4096)
+           for i, (st, ch) in enumerate([("unit", False), ("unit", True), ("integral", False)])]
+    res = _batched(scs, [0, 0, 1], use_graph=use_graph)
+    for i, sc in enumerate(scs):
+        _assert_same(_solo(sc), res[i], f"unit job {i}")
+
+
+@gpu
 def test_batch_matches_alone_two_voices_per_lane_fast_fp():
     scs = _jobs(strict_fp=0, vpl=2)[:3]
     res = _batched(scs, [0, 0, 0])
