@@ -274,7 +274,7 @@ const char* kh_last_error(void);
  * The gate table (src/voice.rs:212-452) on its own, and the bank's DSP
  * helpers, so the reference's in-module tests (src/voice.rs:660-766,
  * src/bank.rs:981-1035, src/resample.rs:109-171) can be restated against
- * this build. */
+ * this library. */
 typedef struct kh_gates kh_gates;
 kh_gates* kh_gates_new(uint32_t block_frames, uint32_t gate_frames);
 void kh_gates_destroy(kh_gates* g);

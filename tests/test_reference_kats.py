@@ -1,4 +1,4 @@
-"""The reference's own known-answer tests, restated against this build.
+"""The reference's own known-answer tests, restated against this library.
 
 Kestrel ships no golden vectors for the backend path (its tests/ directory is
 not distributed, README.md:33-39), only in-module unit tests. Each test here
