@@ -262,9 +262,15 @@ int kh_driver_finish(kh_driver* d, uint64_t active_voices, int* more);
  * another block follows, from the state the last admitted block left, so it
  * may be called after the next block's collect. The order
  *   collect(0) admit(0) advance  [collect(n+1) more(n) admit(n+1) advance]...
- * gives the same blocks and answers as prepare/finish. */
+ * gives the same blocks and answers as prepare/finish, and so does admitting
+ * block n + 1 before more(n) when kh_driver_admit_ready says it may. */
 int kh_driver_collect(kh_driver* d);
 int kh_driver_admit(kh_driver* d, uint32_t live, kh_block* out);
+/* 1 when the collected block's admission does not depend on `live` (every
+ * queued layer fits in what one block may steal): kh_driver_admit may then
+ * run before the previous block's render has ended, with any `live` (the
+ * block's `live` field then reports that value, not the pool's). */
+int kh_driver_admit_ready(const kh_driver* d);
 int kh_driver_advance(kh_driver* d);
 int kh_driver_more(kh_driver* d, uint64_t active_voices, int* more);
 

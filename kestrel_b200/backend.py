@@ -30,6 +30,11 @@ class BlockStats:
 
 
 class CudaSynth:
+    # kc_spawn only stages the commands: the steal, drop and admission happen
+    # on the device in the next render, so a block's inputs may be staged
+    # while the previous block renders without touching its voices or stats.
+    spawn_deferred = True
+
     def __init__(self, cfg: N.KcConfig, pool: np.ndarray, params: np.ndarray, n_regions: int,
                  max_sample_len: int):
         self._lib = N.cuda_lib()

@@ -99,7 +99,10 @@ struct Driver {
     uint64_t notes_total = 0;
     uint32_t last_want = 0, last_take = 0, last_live = 0;
     uint64_t last_want_energy = 0, last_take_energy = 0;
-    bool done_after_admit = false;
+    // What finish() decides the next block by, as each admitted block left
+    // it, by block parity: a pipelined caller may admit block n + 1 before
+    // asking about block n.
+    bool done_after_admit[2] = {false, false};
 
     // Driver::open, src/driver.rs:343-413.
     // The event source is the synthetic stream of `m`, or `file` when given.
@@ -272,6 +275,14 @@ struct Driver {
         chan.refresh_active();
     }
 
+    // Whether this block's admission is the same for every live count: all
+    // queued layers are admitted, however full the pool, when they fit in
+    // what one block may steal (and the rule may steal at all).
+    bool admit_ready() const {
+        const uint32_t want = std::min<uint32_t>((uint32_t)cands.size(), cfg.max_voices);
+        return cfg.steal_rule != KC_STEAL_DROP_NEW ? want <= max_steal() : want == 0;
+    }
+
     void admit(uint32_t live) {
         const uint32_t want = (uint32_t)cands.size();
         const uint32_t take = admit_take(live, want);
@@ -295,7 +306,7 @@ struct Driver {
         }
         materialise(take);
         // What finish() decides the next block by, as of this block.
-        done_after_admit = stream_done && deferred.empty();
+        done_after_admit[block_index & 1] = stream_done && deferred.empty();
     }
 
     // rank_candidates, src/driver.rs:701-742. select_nth_unstable is a
@@ -587,7 +598,7 @@ struct Driver {
     // Driver::next_block's continuation test (src/driver.rs:625-642), on the
     // state the last admitted block left.
     bool more(uint64_t active_voices) {
-        if (!done_after_admit) return true;
+        if (!done_after_admit[(block_index - 1) & 1]) return true;
         if (active_voices > 0) {
             tail_blocks_left = tail_blocks_left > 0 ? tail_blocks_left - 1 : 0;
             return tail_blocks_left != 0;
@@ -1053,6 +1064,8 @@ int kh_driver_admit(kh_driver* h, uint32_t live, kh_block* out) {
     out->take_energy = d.last_take_energy;
     return 0;
 }
+
+int kh_driver_admit_ready(const kh_driver* h) { return h->d->admit_ready() ? 1 : 0; }
 
 int kh_driver_advance(kh_driver* h) {
     h->d->advance();

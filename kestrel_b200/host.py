@@ -115,6 +115,7 @@ HOST_SYMBOLS = {
     "kh_driver_collect": (C.c_int, [_P]),
     "kh_driver_admit": (C.c_int, [_P, C.c_uint32, C.POINTER(KhBlock)]),
     "kh_driver_advance": (C.c_int, [_P]),
+    "kh_driver_admit_ready": (C.c_int, [_P]),
     "kh_driver_more": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int)]),
     "kh_last_error": (C.c_char_p, []),
     "kh_gates_new": (_P, [C.c_uint32, C.c_uint32]),
@@ -536,6 +537,11 @@ class Driver:
             self._lib.kh_driver_variant(self._h, i, C.byref(idx), C.byref(data), C.byref(n))
             out.append((idx.value, data.value, n.value))
         return out
+
+    def admit_ready(self) -> bool:
+        """Whether the collected block's admission is the same for every
+        live count, so it may run before the previous block has rendered."""
+        return bool(self._lib.kh_driver_admit_ready(self._h))
 
     def advance(self) -> None:
         self._lib.kh_driver_advance(self._h)

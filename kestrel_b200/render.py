@@ -42,7 +42,8 @@ class RenderStats:
     latency_frames: int   # the brickwall's delay
     pipelined: bool = False
     # host seconds by phase: collecting events, admission + feeding the
-    # backend, waiting on the backend, limiter + WAV write
+    # backend, waiting on the backend, limiter + WAV write; and how many
+    # blocks were admitted and staged while the block before them rendered
     phases: dict | None = None
 
     @property
@@ -160,22 +161,28 @@ def _serial(drv, synth, lim, wav, cfg, max_frames, on_block, csv=None):
 def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block, csv=None):
     """The same calls as _serial, reordered so the host overlaps the device:
     collect(n + 1) runs while block n renders, and block n's limiter and WAV
-    write run while block n + 1 renders."""
+    write run while block n + 1 renders. When block n + 1's admission cannot
+    depend on how many voices block n leaves (every queued layer fits in what
+    one block may steal), it is admitted and staged while block n renders
+    too, and block n + 1 starts as soon as block n ends."""
     clock = time.perf_counter
-    ph = {"collect": 0.0, "admit_feed": 0.0, "wait": 0.0, "output": 0.0}
+    ph = {"collect": 0.0, "admit_feed": 0.0, "wait": 0.0, "output": 0.0, "early_blocks": 0}
     frames = blocks = peak_voices = 0
     bufs = [np.empty(cfg.block_frames * 2, np.float32) for _ in range(2)]
 
     adm = []   # admission of the blocks in flight, for the diagnostic rows
 
-    def launch(live):
+    def stage(live):
         t = clock()
         kb = drv.admit_raw(live)
-        adm.append((kb.live, kb.want, kb.take, kb.want_energy, kb.take_energy))
+        adm.append([kb.live, kb.want, kb.take, kb.want_energy, kb.take_energy])
         synth.feed_raw(kb, drv.variant_ptrs(kb))
+        ph["admit_feed"] += clock() - t
+
+    def launch(live):
+        stage(live)
         synth.render_begin()
         drv.advance()
-        ph["admit_feed"] += clock() - t
 
     t = clock()
     drv.collect()
@@ -186,9 +193,16 @@ def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block, csv=None):
         t = clock()
         drv.collect()
         t1 = clock()
+        ph["collect"] += t1 - t
+        # (only for a backend whose spawn is staged until its render, so
+        # that staging block n + 1 cannot touch block n's voices or stats)
+        early = getattr(synth, "spawn_deferred", False) and drv.admit_ready()
+        if early:
+            stage(0)    # the live count is filled in below, for the diagnostic row
+            ph["early_blocks"] += 1
+        t1 = clock()
         out = synth.render_end(bufs[blocks & 1])
         t2 = clock()
-        ph["collect"] += t1 - t
         ph["wait"] += t2 - t1
         st = synth.stats()
         peak_voices = max(peak_voices, st.active_voices)
@@ -197,7 +211,12 @@ def _pipelined(drv, synth, lim, wav, cfg, max_frames, on_block, csv=None):
         blocks += 1
         more = drv.more_after(st.active_voices)
         stop = not more or (max_frames and frames >= max_frames)
-        if not stop:
+        if early:
+            adm[-1][0] = st.active_voices
+            if not stop:
+                synth.render_begin()
+                drv.advance()
+        elif not stop:
             launch(st.active_voices)
         t = clock()
         lim.process(out)
@@ -326,7 +345,8 @@ def main(argv=None) -> int:
                      block_csv=args.block_csv, nan_guard=args.nan_guard, progress=None if args.quiet else progress)
     print(f"{st.seconds:.2f} s rendered in {st.wall_s:.2f} s ({st.x_realtime:.2f}x realtime), {st.blocks} blocks, "
           f"peak {st.peak_voices} voices, {st.clipped} samples clipped, {st.data_bytes} bytes"
-          + (", host s: " + ", ".join(f"{k} {v:.2f}" for k, v in st.phases.items()) if st.phases else ""),
+          + (", host s: " + ", ".join(f"{k} {v:.2f}" for k, v in st.phases.items() if k != "early_blocks")
+             + f", {st.phases['early_blocks']} blocks staged early" if st.phases else ""),
           flush=True)
     return 0
 

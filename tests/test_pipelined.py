@@ -87,21 +87,27 @@ def test_split_driver_equals_prepare_finish(tmp_path, workload, over):
         if not more:
             break
     assert len(serial) > 8
-    # pipelined: collect(n + 1) comes before more(n)
-    piped, live = [], 0
+    # pipelined: collect(n + 1) comes before more(n), and so does admit(n + 1)
+    # whenever its admission cannot depend on the live count
+    piped, live, early = [], 0, 0
     b.collect()
     blk = b.admit(live)
     b.advance()
     while True:
         b.collect()
+        nxt = b.admit(0) if b.admit_ready() else None
         live = _decay(live, blk, cfg.max_voices)
         more = b.more_after(live)
         piped.append((blk, more))
         if not more:
             break
-        blk = b.admit(live)
+        if nxt is not None:
+            nxt.live = live       # the caller's live count, which admission did not need
+            blk, early = nxt, early + 1
+        else:
+            blk = b.admit(live)
         b.advance()
-    assert len(piped) == len(serial)
+    assert len(piped) == len(serial) and early > 0
     for (x, mx), (y, my) in zip(serial, piped):
         _same_inputs(x, y)
         assert mx == my
@@ -111,30 +117,42 @@ def test_split_driver_equals_prepare_finish(tmp_path, workload, over):
 
 class _AsyncOracle:
     """The CPU reference backend behind the asynchronous calls, so the
-    pipelined loop's ordering is checked without a GPU."""
+    pipelined loop's ordering is checked without a GPU. Like the CUDA
+    backend, it stages a block's inputs and applies them (the spawn
+    included) only when that block begins."""
+
+    spawn_deferred = True
 
     def __init__(self, cfg, bank):
         from oracle.binding import OracleSynth
         self.o = OracleSynth(cfg, bank.pool, bank.params)
         self.block_frames = cfg.block_frames
         self.held = None
+        self.staged = None
 
     def feed_raw(self, kb, variants):
+        vs = []
         for idx, addr, n in variants:
-            data = np.frombuffer((C.c_char * (n * N.PARAMS_DTYPE.itemsize)).from_address(addr),
-                                 dtype=N.PARAMS_DTYPE).copy()
-            self.o.set_params_variant(idx, data)
-        self.o.set_gates(np.ctypeslib.as_array(kb.gates, shape=(kb.n_gates,)).copy())
-        self.o.set_channels(np.ctypeslib.as_array(kb.chan, shape=(kb.n_chan,)).copy(), bool(kb.bend),
-                            bool(kb.gain), bool(kb.variant))
+            vs.append((idx, np.frombuffer((C.c_char * (n * N.PARAMS_DTYPE.itemsize)).from_address(addr),
+                                          dtype=N.PARAMS_DTYPE).copy()))
+        gates = np.ctypeslib.as_array(kb.gates, shape=(kb.n_gates,)).copy()
+        chan = np.ctypeslib.as_array(kb.chan, shape=(kb.n_chan,)).copy()
         if kb.n_cmds:
             raw = (C.c_char * (kb.n_cmds * N.SPAWN_DTYPE.itemsize)).from_address(kb.cmds)
-            self.o.spawn(np.frombuffer(raw, dtype=N.SPAWN_DTYPE).copy())
+            cmds = np.frombuffer(raw, dtype=N.SPAWN_DTYPE).copy()
         else:
-            self.o.spawn(np.zeros(0, N.SPAWN_DTYPE))
+            cmds = np.zeros(0, N.SPAWN_DTYPE)
+        self.staged = (vs, gates, chan, bool(kb.bend), bool(kb.gain), bool(kb.variant), cmds)
 
     def render_begin(self):
-        assert self.held is None
+        assert self.held is None and self.staged is not None
+        vs, gates, chan, bend, gain, variant, cmds = self.staged
+        self.staged = None
+        for idx, data in vs:
+            self.o.set_params_variant(idx, data)
+        self.o.set_gates(gates)
+        self.o.set_channels(chan, bend, gain, variant)
+        self.o.spawn(cmds)
         self.held = self.o.render()
 
     def render_end(self, out):
@@ -170,13 +188,18 @@ def _oracle(cfg, bank):
 @pytest.mark.parametrize("source", ["synthetic", "smf"])
 def test_pipelined_loop_equals_serial_on_cpu(tmp_path, source):
     cfg, bs, ms = _spec("black", notes=6000, seconds=0.6, cluster_lo=50, cluster_hi=300, program_period_s=0.2,
-                        max_voices=4096)
+                        max_voices=4096, max_steal_percent=5)
     if source == "smf":
         ms = _sound_cc_file(tmp_path / "cc.mid", notes=60)
     a = render_file(tmp_path / "serial.wav", cfg, bs, ms, backend=_oracle)
     b = render_file(tmp_path / "piped.wav", cfg, bs, ms, backend=_tracking_async)
     assert not a.pipelined and b.pipelined and b.phases is not None
     assert (a.blocks, a.peak_voices, a.clipped) == (b.blocks, b.peak_voices, b.clipped)
+    # blocks admitted while the one before rendered, and (with clusters over
+    # the steal budget) blocks that waited for it
+    assert b.phases["early_blocks"] > 0
+    if source == "synthetic":
+        assert b.phases["early_blocks"] < b.blocks - 1
     assert (tmp_path / "serial.wav").read_bytes() == (tmp_path / "piped.wav").read_bytes()
 
 
