@@ -150,16 +150,34 @@ def measured_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def render_traffic_per_unit() -> float | None:
-    """DRAM bytes (read + write) per voice-sample of the render kernel, from the
-    committed ncu summary of that kernel (profiles/render_traffic.json)."""
+def render_profile_per_unit(key: str = "dram_bytes_per_voice_sample") -> float | None:
+    """A per-voice-sample figure of the render kernel from the committed ncu
+    summary of it at this workload (profiles/render_traffic.json): DRAM bytes
+    read + written, or lane instructions issued."""
     p = ROOT / "profiles" / "render_traffic.json"
     if p.exists():
         try:
-            return float(json.loads(p.read_text())["dram_bytes_per_voice_sample"])
+            return float(json.loads(p.read_text())[key])
         except Exception:
             return None
     return None
+
+
+def torch_sm_count() -> int | None:
+    try:
+        import torch
+        return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    except Exception:
+        return None
+
+
+def issue_roofline(lane_instr_per_unit, units, launch_ms, sms, sm_mhz):
+    if not (lane_instr_per_unit and launch_ms and sms and sm_mhz):
+        return None
+    achieved = lane_instr_per_unit * units / 32.0 / (launch_ms * 1e-3)
+    peak = sms * 4 * sm_mhz * 1e6
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp-instr/s", "frac": achieved / peak,
+            "lane_instructions_per_voice_sample": lane_instr_per_unit}
 
 
 # ---- the CUDA arm ------------------------------------------------------------------
@@ -447,7 +465,9 @@ def main(argv=None):
         n_render_mean = r["mean_live"]
         bytes_launch = render_algorithmic_bytes(int(round(n_render_mean)), r["bf"], r["tiles"])
         achieved = bytes_launch / (r["render_ms"] * 1e-3) / 1e9 if r["render_ms"] > 0 else 0.0
-        tpu = render_traffic_per_unit()
+        tpu = render_profile_per_unit()
+        ipu = render_profile_per_unit("lane_instructions_per_voice_sample")
+        sms = torch_sm_count()
         value = units / (ms_t * 1e-3)
         line = {
             "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": K,
@@ -466,6 +486,12 @@ def main(argv=None):
                          "algorithmic_bytes_per_launch": bytes_launch,
                          "launch_ms": r["render_ms"],
                          "traffic": (tpu * n_render_mean * r["bf"]) if tpu else None},
+            # The same launch against instruction issue, its tighter bound: the
+            # profiled instructions per voice-sample x the voice-samples of the
+            # launch / its CUDA-event time, against one warp instruction per
+            # scheduler per cycle (4 per SM) at the SM clock sampled meanwhile.
+            "issue_roofline": issue_roofline(ipu, n_render_mean * r["bf"], r["render_ms"], sms,
+                                             r["clocks"].get("sm_mhz") if r["clocks"] else None),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_units / e2e_s if e2e_s > 0 else 0.0, "unit": unit,
                     "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
