@@ -321,6 +321,55 @@ def run_oracle(workload, seed, threads, max_blocks, max_seconds):
             "sample_rate": cfg.sample_rate}
 
 
+def _served_cpu_job(n_jobs, seed, served_seconds, index, budget_s):
+    """One served job through the CPU restatement of src/cpu.rs, one thread,
+    for at most its block bound or `budget_s` of CPU: (voice-samples, s)."""
+    from kestrel_b200 import host as H
+    from kestrel_b200 import serve as S
+    from oracle.binding import OracleSynth
+    sp = S.served_jobs(n_jobs, seed=seed, max_seconds=served_seconds)[index]
+    bank = H.Bank(sp.bank, sp.cfg, sp.opt)
+    drv = H.Driver(sp.cfg, bank, sp.midi)
+    orc = OracleSynth(sp.cfg, bank.pool, bank.params, threads=1)
+    out = np.empty(sp.cfg.block_frames * 2, np.float32)
+    units, t_sum, blocks = 0, 0.0, 0
+    while (not sp.max_blocks or blocks < sp.max_blocks) and t_sum < budget_s:
+        live = orc.stats().active_voices
+        blk = drv.prepare(live)
+        t0 = time.perf_counter()
+        H.feed(orc, blk)
+        orc.render(out, keep_mix64=False)
+        t_sum += time.perf_counter() - t0
+        units += (live + len(blk.cmds)) * sp.cfg.block_frames
+        blocks += 1
+        if not drv.finish(orc.stats().active_voices):
+            break
+    orc.close()
+    drv.close()
+    return units, t_sum
+
+
+def served_cpu_baseline(n_jobs, seed, served_seconds, workers, budget_s):
+    """The served job mix as independent jobs on `workers` host cores (the
+    CPU baseline of the batched configuration), each job a bounded sample of
+    its render: summed voice-samples over summed render seconds, times the
+    workers that ran at once."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    # spawn: the parent may already hold a CUDA context
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        res = list(ex.map(_served_cpu_job, [n_jobs] * n_jobs, [seed] * n_jobs, [served_seconds] * n_jobs,
+                          range(n_jobs), [budget_s] * n_jobs))
+    units = sum(u for u, _ in res)
+    secs = sum(t for _, t in res)
+    per_core = units / secs if secs > 0 else 0.0
+    return {"value": per_core * min(workers, n_jobs), "unit": "voice-samples/s", "cores": min(workers, n_jobs),
+            "kind": "port",
+            "sample": f"the served mix's {n_jobs} jobs, each rendered by the C++ restatement of src/cpu.rs on one "
+                      f"thread for its first blocks (at most {budget_s:g} s of CPU each), as independent jobs on "
+                      f"{min(workers, n_jobs)} cores: the per-core rate x the cores"}
+
+
 def run_served(args):
     """The batched-and-served configuration: the same seeded job mix through
     the render server twice -- continuous batching (one kc_batch_render per
@@ -380,6 +429,9 @@ def run_served(args):
                                                     "host drivers, host buffers and per-block readback"},
         "clocks": clk,
     }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = served_cpu_baseline(len(jobs), args.seed, args.served_seconds,
+                                                   os.cpu_count() or 1, max(args.cpu_seconds / 10, 0.5))
     return line
 
 

@@ -55,3 +55,11 @@ def test_each_rank_renders_its_own_seeded_job():
     a = H.config_workload("plain", seed=1 + 0)[2]
     b = H.config_workload("plain", seed=1 + 1)[2]
     assert a.seed != b.seed and a.notes == b.notes
+
+
+def test_served_cpu_baseline_runs_jobs_on_separate_cores():
+    """The served configuration's CPU baseline: the job mix through the CPU
+    restatement as independent processes (spawned), a bounded sample each."""
+    import bench
+    r = bench.served_cpu_baseline(2, 1, 0.2, 2, 0.3)
+    assert r["kind"] == "port" and r["cores"] == 2 and r["value"] > 0
