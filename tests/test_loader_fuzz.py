@@ -68,3 +68,35 @@ def test_damaged_files_load_or_are_refused(tmp_path, fmt):
         except (RuntimeError, OSError, ValueError):
             refused += 1
     assert loaded + refused == 150 and loaded > 0
+
+
+def test_driver_over_damaged_midi_files(tmp_path):
+    """The block driver over damaged MIDI files with programs, controllers,
+    tempo changes and bends: each opens and runs, or is refused."""
+    rng = random.Random(21)
+    cfg, bs, _ = H.config_workload("plain", seed=1)
+    bank = H.Bank(bs, cfg)
+    tr = b""
+    for i in range(40):
+        tr += TS.vlq(5) + bytes([0xC0 | (i % 16), i % 128]) + TS.vlq(0) + bytes([0xB0 | (i % 16), 7, 100])
+        tr += TS.vlq(0) + b"\xff\x51\x03" + struct.pack(">I", 300000 + i * 1000)[1:]
+        tr += TS.vlq(3) + bytes([0x90 | (i % 16), 30 + i, 90]) + TS.vlq(0) + bytes([0xE0 | (i % 16), 0, 64 + i])
+        tr += TS.vlq(7) + bytes([0x80 | (i % 16), 30 + i, 0])
+    tr += TS.vlq(0) + b"\xff\x2f\x00"
+    mid = TS.smf([tr, TS.vlq(0) + b"\xff\x2f\x00"])
+    ran = 0
+    for _ in range(60):
+        (tmp_path / "m.mid").write_bytes(_mutate(rng, mid))
+        try:
+            drv = H.Driver(cfg, bank, tmp_path / "m.mid")
+        except RuntimeError:
+            continue
+        live = 0
+        for _ in range(40):
+            blk = drv.prepare(live)
+            live = min(cfg.max_voices, live + len(blk.cmds)) // 2
+            if not drv.finish(live):
+                break
+        drv.close()
+        ran += 1
+    assert ran > 40
