@@ -50,7 +50,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-PREROLL = {"steal": 64, "black": 48, "plain": 24}
+PREROLL = {"steal": 64, "steal-bent": 64, "black": 48, "plain": 24}
 
 
 def parse_args(argv=None):
@@ -59,7 +59,7 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--workload", choices=["steal", "black", "plain", "served"], default="steal")
+    ap.add_argument("--workload", choices=["steal", "steal-bent", "black", "plain", "served"], default="steal")
     ap.add_argument("--served-jobs", type=int, default=32, help="jobs of the served workload")
     ap.add_argument("--served-seconds", type=float, default=2.0,
                     help="audio seconds rendered per served job (its MIDI keeps its full length)")
@@ -70,6 +70,7 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound of the cpu_baseline sample")
     ap.add_argument("--voices-per-lane", type=int, default=0)
     ap.add_argument("--strict-fp", type=int, default=1)
+    ap.add_argument("--mix-mode", type=int, default=0, help="0 f32 tree, 1 compensated two-sum, 2 FP64")
     return ap.parse_args(argv)
 
 
@@ -193,6 +194,7 @@ def run_cuda(args, world, rank, local):
     cfg.device = local
     cfg.voices_per_lane = args.voices_per_lane
     cfg.strict_fp = args.strict_fp
+    cfg.mix_mode = args.mix_mode
     bank = H.Bank(bs, cfg)
     drv = H.Driver(cfg, bank, ms)
     A = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)
@@ -450,6 +452,9 @@ def workload_desc(name):
     return {
         "steal": "steal-saturation: 200M notes / 120 s, log-normal durations (median 6 s, sigma 0.5), "
                  "1 preset x 128 zones, max_voices 8,388,608, steal-percent 10",
+        "steal-bent": "steal-saturation with a pitch-bend, CC7 and CC11 curve per channel every 10 ms (every voice "
+                      "at a fractional step): 200M notes / 120 s, log-normal durations (median 6 s, sigma 0.5), "
+                      "1 preset x 128 zones, max_voices 8,388,608, steal-percent 10",
         "black": "black-midi: 20M notes / 180 s, 60% in 1 ms clusters of 1k-50k, 128 presets, "
                  "bend+CC7+CC11 every 10 ms, max_voices 1,048,576",
         "plain": "plain: 100k notes / 30 s, 1 preset, max_voices 65,536",
@@ -531,7 +536,7 @@ def main(argv=None):
                        "mean_voices_rendered": round(n_render_mean), "preroll_blocks": r["preroll"],
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (voice pool >= 1.8 GB at 8.4M voices)"
-                             if args.workload == "steal" else "inputs smaller than L2 between blocks",
+                             if args.workload.startswith("steal") else "inputs smaller than L2 between blocks",
                        "replay_equals_host_render": r["same"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_render",

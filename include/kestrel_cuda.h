@@ -129,7 +129,7 @@ typedef struct kc_config {
     uint32_t gate_frames;        /* gate/controller tile, 32; a multiple of 16 or a divisor of 16 */
     uint32_t max_voices;         /* pool ceiling surviving a block */
     uint32_t max_steal_percent;  /* 1..=100, 25 */
-    uint32_t steal_fade_frames;  /* 1..block_frames, 96 */
+    uint32_t steal_fade_frames;  /* 1..block_frames-1, 96 */
     uint32_t steal_rule;         /* KC_STEAL_*, Quietest */
     uint32_t admit_rule;         /* KC_ADMIT_*, Loudest */
     uint32_t interpolation;      /* KC_INTERP_*, Linear */
@@ -285,6 +285,19 @@ int kc_resample_i16_batch(void* device, uint32_t n, const int16_t* const* src, c
  * and updating the voices' state in place. All pointers are device pointers;
  * `d_params` holds `n_slots` copies of `params_len` entries; `stream` is a
  * cudaStream_t (NULL: the legacy default stream). The call only enqueues work.
+ * `d_params` and `d_chan` must be 16-byte aligned, `d_pool`, `d_gates` and
+ * `d_out` 4-byte aligned (KC_ERR_INVALID otherwise). The mix is KC_MIX_F32_TREE
+ * or KC_MIX_TWO_SUM; KC_MIX_F64 is refused.
+ *
+ * It renders from the i16 sample pool the caller passes, converting each tap,
+ * and a voice that dies mid-block keeps its lane idle for the rest of the
+ * block (kc_render instead renders from an f32 copy of the pool and turns
+ * dead voices into silent lanes that keep their warp on the fast paths), so
+ * it is slower per voice than kc_render; the output is the same within the
+ * mix's tolerance. Device-side range errors are not reported: a voice whose
+ * params index is past `params_len` or whose gate slot is past
+ * KC_GATE_SLOTS renders with entry 0 or slot 0 (kc_render reports both as
+ * KC_ERR_DEVICE; its kc_spawn refuses such commands up front).
  *
  * Its scratch (the partial-mix slices and control words) is a 32 MiB
  * file-scope device array that every GPU loading this library holds until the

@@ -684,6 +684,7 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         ra.cap = s->cap;
         ra.pcm = s->pcm;
         ra.pcmf = s->pcmf;
+        ra.pcmp = s->pcmp;
         ra.pcm_len = (uint32_t)std::min<uint64_t>(s->pcm_len, 0xFFFFFFFFull);
         ra.params = s->params;
         ra.params_per = s->params_per;

@@ -56,6 +56,7 @@ constexpr uint32_t SEL_ROUNDS = 8;  // 64-bit key, 8-bit digits
 constexpr uint32_t ERR_PARAMS_RANGE = 1u << 0;
 constexpr uint32_t ERR_SELECT = 1u << 1;
 constexpr uint32_t ERR_COMPACT = 1u << 2;
+constexpr uint32_t ERR_SLOT_RANGE = 1u << 3;
 
 // Per-block control words, written by the host (or by a staging kernel for the
 // device-resident form) before the block's kernels run.
@@ -88,7 +89,7 @@ struct DevState {
 };
 
 // 64-bit step scaled by an 8.24 factor, truncating, saturating
-// (fixed.rs:140-148; the device form of shaders/common.wgsl:204-216).
+// (Fixed::scale, src/fixed.rs:83-90; the device form of shaders/common.wgsl:198-216).
 __device__ __forceinline__ uint64_t scale_step(uint64_t v, uint32_t factor) {
     const uint64_t lo = v * (uint64_t)factor;       // product bits 0..63
     const uint64_t hi = __umul64hi(v, (uint64_t)factor);  // bits 64..95

@@ -38,7 +38,7 @@ inline I sat_cast(F v) {
 // f32::round / f64::round: half away from zero (std::round does the same).
 inline float rroundf(float v) { return std::round(v); }
 
-// Fixed::from_f64 (src/fixed.rs:83-96).
+// Fixed::from_f64 (src/fixed.rs:24-38).
 inline uint64_t fixed_from_f64(double v) {
     const double scaled = v * 4294967296.0;
     if (std::isnan(scaled) || scaled <= 0.0) return 0;
@@ -46,7 +46,7 @@ inline uint64_t fixed_from_f64(double v) {
     return (uint64_t)scaled;
 }
 
-// bend_factor (src/fixed.rs:157-171).
+// bend_factor (src/fixed.rs:101-113).
 inline uint32_t bend_factor(double semitones) {
     if (!std::isfinite(semitones)) return 1u << 24;
     const double f = std::exp2(semitones / 12.0) * (double)(1u << 24);

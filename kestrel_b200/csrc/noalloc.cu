@@ -188,13 +188,23 @@ int kc_render_block_noalloc(const kc_config* cfg, uint32_t* d_pool, uint32_t cap
     if (c.gate_frames == 0 || c.gate_frames % kc::MIX_TILE != 0 || c.block_frames % c.gate_frames != 0)
         return fail(KC_ERR_INVALID, "gate_frames must be a multiple of 16 that divides block_frames");
     if (c.steal_fade_frames == 0 || c.steal_fade_frames >= c.block_frames)
-        return fail(KC_ERR_INVALID, "steal_fade_frames must be in 1..block_frames");
-    if (c.interpolation > 2 || c.decay_curve > 1 || c.release_curve > 1 || c.mix_mode > 1)
+        return fail(KC_ERR_INVALID, "steal_fade_frames must be in 1..block_frames-1");
+    if (c.interpolation > 2 || c.decay_curve > 1 || c.release_curve > 1 || c.mix_mode > 2)
         return fail(KC_ERR_INVALID, "unknown enum value in config");
+    if (c.mix_mode == KC_MIX_F64)
+        return fail(KC_ERR_INVALID, "KC_MIX_F64 is not supported by kc_render_block_noalloc (its f64 slices would "
+                                    "halve the voices the scratch holds); use KC_MIX_F32_TREE or KC_MIX_TWO_SUM");
     if (n_voices > cap) return fail(KC_ERR_INVALID, "n_voices exceeds the pool's field stride (cap)");
     if ((n_voices && !d_pool) || !d_gates || !d_chan || !d_out || !d_params || params_len == 0 || n_slots == 0)
         return fail(KC_ERR_INVALID, "null or empty argument");
     if (pcm_len && !d_pcm) return fail(KC_ERR_INVALID, "null sample pool");
+    // The kernels read params records and channel rows as 16-byte vectors and
+    // the pool, gate rows and output as 32-bit words.
+    const auto misaligned = [](const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) != 0; };
+    if (misaligned(d_params, 16) || misaligned(d_chan, 16))
+        return fail(KC_ERR_INVALID, "d_params and d_chan must be 16-byte aligned");
+    if (misaligned(d_pool, 4) || misaligned(d_gates, 4) || misaligned(d_out, 4) || misaligned(d_pcm, 2))
+        return fail(KC_ERR_INVALID, "d_pool, d_gates and d_out must be 4-byte aligned, d_pcm 2-byte aligned");
     const uint32_t max_voices = noalloc_max_voices(c);
     if (n_voices > max_voices)
         return fail(KC_ERR_INVALID, "n_voices " + std::to_string(n_voices) +
@@ -240,8 +250,8 @@ int kc_render_block_noalloc(const kc_config* cfg, uint32_t* d_pool, uint32_t cap
         void* fn = render_pick(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode);
         void* args[] = {&ra};
         const unsigned ctas = (nbatch + kc::RENDER_WARPS - 1) / kc::RENDER_WARPS;
-        // 8 warp tiles of 16 x 72 floats = 36,864 bytes: under the 48 KiB
-        // every kernel may take without an opt-in attribute.
+        // 8 warp areas of SM_WARP (1,224) floats = 39,168 bytes: under the
+        // 48 KiB every kernel may take without an opt-in attribute.
         const size_t smem = (size_t)kc::RENDER_WARPS * kc::SM_WARP * sizeof(float);
         cudaError_t e = cudaLaunchKernel(fn, dim3(ctas), dim3(kc::RENDER_WARPS * 32), args, smem, q);
         if (e != cudaSuccess) return fail(KC_ERR_CUDA, std::string("render launch: ") + cudaGetErrorString(e));

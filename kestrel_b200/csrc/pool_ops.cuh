@@ -135,7 +135,7 @@ __device__ __forceinline__ void select_refine_body(PoolArgs a, const uint32_t* s
 }
 
 // Schedule each victim's fade (src/cpu.rs:360-371; shaders/compact.wgsl:
-// 263-291): stop_rel = (note id low word) % span + 1. Only the pre-spawn
+// 148-179): stop_rel = (note id low word) % span + 1. Only the pre-spawn
 // voices are candidates.
 __device__ __forceinline__ void mark_stolen_body(PoolArgs a, uint32_t cta, uint32_t ctas) {
     const DevState* st = a.st;
@@ -284,7 +284,7 @@ __device__ __forceinline__ void copy_voice(const uint32_t* src, uint32_t* dst, u
 #pragma unroll
     for (uint32_t f = 0; f < VOICE_FIELDS; ++f) dst[f * cap + to] = src[f * cap + from];
     // Start offset, born-under variant and stop frame apply only to the block
-    // a voice was born or stolen in (shaders/compact.wgsl:245-249).
+    // a voice was born or stolen in (shaders/compact.wgsl:134-138).
     dst[F_START_REL * cap + to] = 0u;
     dst[F_BORN_VARIANT * cap + to] = 0u;
     dst[F_STOP_REL * cap + to] = 0u;

@@ -42,6 +42,7 @@ struct RenderArgs {
     const int16_t* pcm;        // sample pool, i16 as the bank holds it
     const float* pcmf;         // the same pool converted once to f32 (F32 kernels), followed
                                // by ZERO_PAD zero frames (the taps of neutral lanes)
+    const float2* pcmp;        // per frame of pcmf: (tap, (next tap - tap) * 2^-32) (F32 kernels)
     uint32_t pcm_len;          // frames in it
     const kc_region_params* params;  // n_slots copies of params_per
     uint32_t params_per;
@@ -508,6 +509,14 @@ __device__ __forceinline__ void load_voice(VoiceRegs& v, const RenderArgs& a, ui
     v.born = P[F_BORN_VARIANT * cap];
     v.stop_rel = P[F_STOP_REL * cap];
     v.variant = v.born ? v.born - 1u : 0u;
+    // A pool the caller owns (kc_render_block_noalloc) may hold indexes that
+    // kc_spawn's validation never saw: an out-of-range gate slot or params
+    // index raises an error bit and reads slot / entry 0 instead of reading
+    // past its table.
+    if (v.slot >= KC_GATE_SLOTS) {
+        atomicOr(&a.st->error, ERR_SLOT_RANGE);
+        v.slot = 0;
+    }
     v.channel = (v.slot >> 7) & 15u;
     v.born_gate = v.start_rel / a.gate_frames;
     if (v.params_base >= a.params_per) {
@@ -720,6 +729,35 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
         }
 #pragma unroll
         for (int k = 0; k < V; ++k) v[k].phase += v[k].step << LOG_NT;
+    } else if constexpr (F32) {
+        // The tap index rides in the high word of q = phase + (base << 32)
+        // (fast_ok proved base + index + 1 < pcm_len, so it cannot carry out),
+        // and one 64-bit load fetches the pair (s0, d') with
+        // d' = (s1 - s0) * 2^-32 from the tap-pair table. Then
+        // d' * f32(lo) == (s1 - s0) * (f32(lo) * 2^-32) exactly -- the
+        // power-of-two scale commutes with the rounding, nothing here is
+        // subnormal -- so s0 + that is the reference's interpolation
+        // (src/cpu.rs:279-283) bit for bit, in three operations instead of
+        // five and one load instead of two.
+        uint64_t q[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) q[k] = v[k].phase + ((uint64_t)v[k].base << 32);
+#pragma unroll
+        for (uint32_t i = 0; i < NT; ++i) {
+            float y[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
+                const float2 t = __ldg(a.pcmp + (uint32_t)(q[k] >> 32));
+                const float fl = __uint2float_rn((uint32_t)q[k]);
+                const float s = STRICT ? __fadd_rn(t.x, __fmul_rn(t.y, fl)) : __fmaf_rn(t.y, fl, t.x);
+                y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(s, v[k].level));
+                q[k] += v[k].step;
+            }
+            emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) v[k].phase = q[k] - ((uint64_t)v[k].base << 32);
     } else {
 #pragma unroll
         for (uint32_t i = 0; i < NT; ++i) {

@@ -100,6 +100,20 @@ __global__ void __launch_bounds__(256) k_convert_pool(const int16_t* __restrict_
         pcmf[i] = fmaxf(__fmul_rn((float)pcm[i], 1.0f / 32767.0f), -1.0f);
 }
 
+// The fractional path's tap pairs, from the f32 copy (and its zero pad):
+// entry i = (s_i, (s_{i+1} - s_i) * 2^-32). The difference is rounded once,
+// as the reference rounds `s1 - s0`, and the power-of-two scale is exact, so
+// (d * 2^-32) * f32(lo) is the reference's (s1 - s0) * (lo as f32 * 2^-32)
+// bit for bit (render.cuh, hot_tile). Entries past the pool pair zeros.
+__global__ void __launch_bounds__(256) k_pair_pool(const float* __restrict__ pcmf, float2* __restrict__ pcmp,
+                                                   uint64_t n, uint64_t n_pad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float s0 = i < n ? pcmf[i] : 0.0f;
+        const float s1 = i + 1 < n ? pcmf[i + 1] : 0.0f;
+        pcmp[i] = make_float2(s0, __fmul_rn(__fsub_rn(s1, s0), 2.3283064365386963e-10f));
+    }
+}
+
 }  // namespace kc
 
 using namespace kc;
@@ -211,6 +225,7 @@ void free_all(kc_synth* s) {
     cudaFree(s->pool[1]);
     cudaFree(s->pcm);
     cudaFree(s->pcmf);
+    cudaFree(s->pcmp);
     cudaFree(s->params);
     cudaFree(s->gates);
     cudaFree(s->chan);
@@ -250,7 +265,7 @@ int validate(const kc_config& c) {
         return fail(KC_ERR_INVALID, "gate_frames must be a multiple of 16 that divides block_frames");
     if (c.max_voices == 0) return fail(KC_ERR_INVALID, "max_voices must be non-zero");
     if (c.steal_fade_frames == 0 || c.steal_fade_frames >= c.block_frames)
-        return fail(KC_ERR_INVALID, "steal_fade_frames must be in 1..block_frames");
+        return fail(KC_ERR_INVALID, "steal_fade_frames must be in 1..block_frames-1");
     if (c.max_steal_percent == 0 || c.max_steal_percent > 100)
         return fail(KC_ERR_INVALID, "max_steal_percent must be in 1..=100");
     if (c.steal_rule > 2 || c.admit_rule > 1 || c.interpolation > 2 || c.decay_curve > 1 ||
@@ -317,6 +332,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     ra.cap = s->cap;
     ra.pcm = s->pcm;
     ra.pcmf = s->pcmf;
+    ra.pcmp = s->pcmp;
     ra.pcm_len = (uint32_t)std::min<uint64_t>(s->pcm_len, 0xFFFFFFFFull);
     ra.params = s->params;
     ra.params_per = s->params_per;
@@ -406,7 +422,7 @@ uint64_t footprint(const kc_config& c, uint64_t cap, uint64_t pcm_len, uint64_t 
     const uint64_t samples = (uint64_t)c.block_frames * 2;
     uint64_t n = 2ull * VOICE_FIELDS * cap * 4;                                 // pool, double-buffered
     n += std::max<uint64_t>(pcm_len, 1) * 2 + 64;                               // sample pool (i16)
-    n += (pcm_len + ZERO_PAD) * 4;                                               // its f32 copy + zero pad
+    n += (pcm_len + ZERO_PAD) * 12;                                              // its f32 copy and tap pairs
     n += params_per * sizeof(kc_region_params) * n_slots;                       // params variants
     n += (uint64_t)tiles * (KC_GATE_SLOTS + KC_BEND_CHANNELS * KC_CHAN_FIELDS) * 4;
     n += (uint64_t)cmds_cap * sizeof(kc_spawn_cmd) + samples * 4;               // spawn buffer, block
@@ -534,6 +550,10 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
                          s->stream>>>(s->pcm, s->pcmf, pool_len);
         KC_TRY(cudaGetLastError());
     }
+    KC_TRY(cudaMalloc(&s->pcmp, (pool_len + ZERO_PAD) * sizeof(float2)));
+    k_pair_pool<<<(unsigned)std::min<uint64_t>((pool_len + ZERO_PAD + 255) / 256, (uint64_t)s->sms * 16), 256, 0,
+                  s->stream>>>(s->pcmf, s->pcmp, pool_len, pool_len + ZERO_PAD);
+    KC_TRY(cudaGetLastError());
     const size_t per_bytes = (size_t)params_len * sizeof(kc_region_params);
     KC_TRY(cudaMalloc(&s->params, per_bytes * s->n_slots));
     // Every slot starts as a copy of the bank's table, which is what

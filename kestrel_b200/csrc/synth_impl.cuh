@@ -33,6 +33,7 @@ struct kc_synth {
     int parity = 0;
     int16_t* pcm = nullptr;
     float* pcmf = nullptr;      // the pool converted to f32 once (k_convert_pool)
+    float2* pcmp = nullptr;     // per frame: (tap, (next tap - tap) * 2^-32), the fractional path's taps
     kc_region_params* params = nullptr;
     uint32_t* gates = nullptr;
     uint32_t* chan = nullptr;

@@ -624,10 +624,14 @@ def config_workload(name: str, seed: int = 1):
         ms = midi_spec(notes=20_000_000, seconds=180.0, dur_median_s=0.080, dur_sigma=1.0, cluster_share=0.6,
                        cluster_lo=1000, cluster_hi=50000, cc_period_ms=10.0, program_period_s=2.0, programs=128,
                        seed=seed)
-    elif name == "steal":
+    elif name in ("steal", "steal-bent"):
         cfg = N.default_config(max_voices=8_388_608, max_steal_percent=10)
         bs = bank_spec(presets=1, seed=seed)
-        ms = midi_spec(notes=200_000_000, seconds=120.0, dur_median_s=6.0, dur_sigma=0.5, seed=seed)
+        # steal-bent: the same notes with a pitch-bend, CC7 and CC11 curve per
+        # channel every 10 ms, so every voice steps by a fractional ratio that
+        # changes each gate tile (the interpolating path real soundfonts take).
+        ms = midi_spec(notes=200_000_000, seconds=120.0, dur_median_s=6.0, dur_sigma=0.5, seed=seed,
+                       cc_period_ms=10.0 if name == "steal-bent" else 0.0)
     else:
         raise ValueError(f"unknown workload {name!r}")
     return cfg, bs, ms

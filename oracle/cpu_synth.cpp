@@ -48,7 +48,7 @@ inline uint32_t f32_as_u32(float v) {
 
 // ---- fixed.rs ---------------------------------------------------------------
 
-// Fixed::scale, src/fixed.rs:140-148: (u128 product) >> 24, saturating.
+// Fixed::scale, src/fixed.rs:83-90: (u128 product) >> 24, saturating.
 inline uint64_t fixed_scale(uint64_t v, uint32_t factor) {
     unsigned __int128 p = ((unsigned __int128)v * factor) >> 24;
     if (p > (unsigned __int128)UINT64_MAX) return UINT64_MAX;
@@ -403,7 +403,7 @@ uint32_t ko_admit_take(const kc_config* c, uint32_t live, uint32_t queued) {
     return std::min(want, cap - (live - need));
 }
 
-// Fixed::from_f64, src/fixed.rs:83-96.
+// Fixed::from_f64, src/fixed.rs:24-38.
 uint64_t ko_fixed_from_f64(double v) {
     double scaled = v * 18446744073709551616.0 / 4294967296.0;
     if (std::isnan(scaled) || scaled <= 0.0) return 0;
@@ -411,7 +411,7 @@ uint64_t ko_fixed_from_f64(double v) {
     return (uint64_t)scaled;
 }
 uint64_t ko_fixed_scale(uint64_t v, uint32_t factor) { return fixed_scale(v, factor); }
-// bend_factor, src/fixed.rs:157-171.
+// bend_factor, src/fixed.rs:101-113.
 uint32_t ko_bend_factor(double semitones) {
     if (!std::isfinite(semitones)) return 1u << 24;
     double f = std::exp2(semitones / 12.0) * (double)(1u << 24);

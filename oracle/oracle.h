@@ -10,7 +10,7 @@
  * Parity pinning: the reference ships no golden vectors for this path (its
  * tests/ directory is git-ignored, src/README.md:33-39), so this restatement
  * is pinned against the reference's own in-module known-answer tests
- * (src/fixed.rs:115-167, src/voice.rs:660-766, src/bank.rs:981-1035,
+ * (src/fixed.rs:116-167, src/voice.rs:660-766, src/bank.rs:981-1035,
  * src/resample.rs:109-171) and against analytic known answers (a looped sine
  * with an instant envelope renders to exactly the sample, src/testkit.rs:318).
  * The Rust crate itself cannot be built here (no cargo/rustc), so block-level

@@ -1,19 +1,31 @@
-"""Parity at the benchmark's full size: the steal-saturation configuration
-with its 8,388,608-voice pool.
+"""Parity at the benchmark configurations' full sizes.
 
-The oracle cannot pre-roll 8.4M voices (minutes per block), so the device
-context renders the pre-roll alone; its pool at the steady state (read back
-between blocks) and its counters are handed to the oracle, and the next block
-is rendered by both from the driver's identical inputs. Compared: live,
-stolen and dropped counts; the surviving pools field by field, matched by
-note id (the device re-sorts its pool); and the audio. An 8.4M-voice mix
-with no limiter peaks hundreds of times above full scale, where one f32
-rounding step of the output alone is about -90 dBFS, so the mix is nulled
-relative to its peak (<= -100 dB), and -- the reference's own criterion, a
-null of the written file -- after the default brickwall output stage, which
-brings the block back under full scale: <= -100 dBFS. The oracle's voice
-loop runs on every host thread (its f64 chunk sums are added in chunk order;
-the tolerance absorbs the summation order).
+The oracle cannot pre-roll millions of voices (minutes per block), so the
+device context renders the pre-roll alone; its pool (read back between
+blocks), its counters and every params variant the driver has handed it are
+then given to the oracle, and the next block is rendered by both from the
+driver's identical inputs. Compared: live, stolen and dropped counts; the
+surviving pools field by field, matched by note id (the device re-sorts its
+pool); and the audio.
+
+* Steal saturation (8,388,608-voice pool, steal-percent 10), default f32
+  tree mix. An 8.4M-voice mix with no limiter peaks hundreds of times above
+  full scale, where one f32 rounding step of the output alone is about
+  -90 dBFS, so the mix is nulled relative to its peak (<= -100 dB), and --
+  the reference's own criterion, a null of the written file -- after the
+  default brickwall output stage, which brings the block back under full
+  scale: <= -100 dBFS.
+* The same block with the compensated two-sum mix (KC_MIX_TWO_SUM): the
+  CUDA block must equal the oracle's own f32 output -- its f64 mix rounded to
+  f32 (src/cpu.rs:615-625) -- to within one f32 ulp on every sample, the
+  closest any f32 output can come to it.
+* Black-MIDI (config 2: 1,048,576-voice pool, 128 presets, bend, CC7 and CC11
+  every 10 ms, program changes): the channel path, the params-variant reload
+  and the select on a 128-preset key layout at the configuration's own pool
+  size, the handover block taken just after a burst.
+
+The oracle's voice loop runs on every host thread (its f64 chunk sums are
+added in chunk order; the tolerances absorb the summation order).
 """
 import os
 
@@ -46,41 +58,68 @@ def test_load_pool_round_trips_without_a_device():
     orc.close()
 
 
-@gpu
-def test_steal_saturation_block_at_full_size():
+def _handover(cfg, bs, ms, until, max_blocks):
+    """Pre-roll the CUDA backend until `until(stats, block_inputs)` holds,
+    then hand its state to the oracle and render one more block on both.
+    Returns (cuda stats before, cuda out, oracle, cuda backend, stats)."""
     from kestrel_b200.backend import CudaSynth
     from oracle.binding import OracleSynth
-    cfg, bs, ms = H.config_workload("steal", seed=3)
     bank = H.Bank(bs, cfg)
     drv = H.Driver(cfg, bank, ms)
     cu = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)
-    # Pre-roll until the pool is saturated and stealing (about 65 blocks, the
-    # benchmark's pre-roll), then one more block of steady state.
-    steady = 0
-    for _ in range(120):
-        H.feed(cu, drv.prepare(cu.stats().active_voices))
+    variants = {}
+    for _ in range(max_blocks):
+        blk = drv.prepare(cu.stats().active_voices)
+        for idx, data in blk.variants:
+            variants[idx] = data
+        H.feed(cu, blk)
         cu.render()
         drv.finish(cu.stats().active_voices)
-        steady += cu.stats().stolen > 0
-        if steady == 2:
+        if until(cu.stats(), blk):
             break
+    else:
+        pytest.fail("the pre-roll never reached the handover state")
     st0 = cu.stats()
-    assert st0.active_voices == cfg.max_voices and st0.stolen > 0
     orc = OracleSynth(cfg, bank.pool, bank.params, threads=os.cpu_count() or 1)
+    for idx, data in variants.items():
+        orc.set_params_variant(idx, data)
     orc.load_pool(cu.read_pool(), st0.stolen, st0.dropped)
     blk = drv.prepare(st0.active_voices)
-    assert len(blk.cmds) > 100_000
     H.feed(cu, blk)
     H.feed(orc, blk)
     out_c = cu.render().copy()
-    out_o = orc.render()
+    out_o = orc.render().copy()
     sc, so = cu.stats(), orc.stats()
     assert (sc.active_voices, sc.stolen, sc.dropped) == (so.active_voices, so.stolen, so.dropped)
-    assert sc.stolen > st0.stolen  # this block stole
     ic, pc = _by_note(cu.read_pool())
     io, po = _by_note(orc.read_pool())
     assert np.array_equal(ic, io), "live sets differ"
     np.testing.assert_array_equal(pc, po)
+    drv.close()
+    return st0, blk, out_c, out_o, orc, cu
+
+
+def _steal_handover(mix_mode):
+    cfg, bs, ms = H.config_workload("steal", seed=3)
+    cfg.mix_mode = mix_mode
+    # Pre-roll until the pool is saturated and has stolen in two blocks
+    # (about 65 blocks, the benchmark's pre-roll); the next block steals too.
+    seen = []
+
+    def until(st, blk):
+        seen.append(st.stolen > 0)
+        return sum(seen) == 2
+
+    st0, blk, out_c, out_o, orc, cu = _handover(cfg, bs, ms, until, 120)
+    assert st0.active_voices == cfg.max_voices and st0.stolen > 0
+    assert len(blk.cmds) > 100_000
+    assert cu.stats().stolen > st0.stolen  # this block stole
+    return out_c, out_o, orc, cu
+
+
+@gpu
+def test_steal_saturation_block_at_full_size():
+    out_c, out_o, orc, cu = _steal_handover(N.MIX_F32_TREE)
     peak = float(np.max(np.abs(orc.last_mix64)))
     assert null_db(out_c, orc.last_mix64) - 20 * np.log10(peak) <= -100.0
     wav_c, wav_o = out_c.copy(), np.array(out_o, np.float32)
@@ -88,5 +127,33 @@ def test_steal_saturation_block_at_full_size():
     H.Limiter().process(wav_o)
     assert np.max(np.abs(wav_c)) <= 1.0 and np.any(wav_c != 0)
     assert null_db(wav_c, wav_o) <= -100.0
+    cu.close()
+    orc.close()
+
+
+@gpu
+def test_steal_saturation_two_sum_block_is_within_one_ulp_of_the_oracle():
+    out_c, out_o, orc, cu = _steal_handover(N.MIX_TWO_SUM)
+    ulp = np.spacing(np.abs(out_o).astype(np.float32))
+    diff = np.abs(out_c.astype(np.float64) - out_o.astype(np.float64))
+    assert np.all(diff <= ulp), f"{int(np.sum(diff > ulp))} samples beyond one ulp, worst {float(np.max(diff / ulp))}"
+    assert float(np.max(np.abs(out_o))) > 10.0  # a mix far above full scale
+    cu.close()
+    orc.close()
+
+
+@gpu
+def test_black_midi_block_at_full_size():
+    cfg, bs, ms = H.config_workload("black", seed=4)
+    assert cfg.max_voices == 1_048_576
+    # Hand over on the block after the first one that admits a burst of more
+    # than 20,000 notes (60% of onsets come in 1 ms clusters of 1k-50k).
+    def until(st, blk):
+        return len(blk.cmds) > 20_000
+
+    st0, blk, out_c, out_o, orc, cu = _handover(cfg, bs, ms, until, 200)
+    assert blk.bend and blk.gain  # the channel path is on
+    assert st0.active_voices > 20_000
+    assert null_db(out_c, orc.last_mix64) <= -100.0
     cu.close()
     orc.close()

@@ -18,15 +18,19 @@ from oracle import binding as O
 FRAC_ONE = 1 << 32
 
 
-# ---- src/fixed.rs:173-224 ------------------------------------------------------
+# ---- src/fixed.rs:116-167 --------------------------------------------------------
+# The module's other two tests -- frac_matches_shader_expression (:147-153)
+# and f32_phase_would_have_failed (:155-166) -- are restated through both
+# backends' render paths in tests/test_analytic.py, where the fraction and the
+# 32.32 phase come out of the oracle's and the device's own arithmetic.
 
-def test_fixed_round_trip_unity():  # fixed.rs:177-183
+def test_fixed_round_trip_unity():  # fixed.rs:119-126
     f = O.lib().ko_fixed_from_f64(1.0)
     assert f >> 32 == 1 and f & 0xFFFFFFFF == 0
     assert np.float32(f & 0xFFFFFFFF) * np.float32(1.0 / 4294967296.0) == 0.0
 
 
-def test_fixed_accumulates_without_drift():  # fixed.rs:185-203
+def test_fixed_accumulates_without_drift():  # fixed.rs:127-145
     ratio = 44100.0 / 48000.0
     step = O.lib().ko_fixed_from_f64(ratio)
     p = 0
@@ -39,27 +43,13 @@ def test_fixed_accumulates_without_drift():  # fixed.rs:185-203
     assert abs(err) < 1.0
 
 
-def test_frac_matches_shader_expression():  # fixed.rs:205-211
-    # The oracle and the device both form frac as f32(lo) * 2^-32.
-    for lo in [0, 1, 0x40000000, 0x80000000, 0xFFFFFFFF]:
-        want = np.float32(lo) * np.float32(1.0 / 4294967296.0)
-        assert np.float32(np.float32(lo) * np.float32(2.0 ** -32)) == want
+# ---- our own checks of src/fixed.rs:72-113 ------------------------------------------
+# The reference has no unit test for Fixed::scale or bend_factor. These assert
+# what their doc comments state (src/fixed.rs:72-82: truncating, saturating
+# 8.24 scaling; :98-100: the 8.24 factor of a bend, BEND_ONE for a non-finite
+# bend) against the oracle's restatement.
 
-
-def test_f32_phase_would_have_failed():  # fixed.rs:213-224
-    p = np.float32(0.0)
-    step = np.float32(44100.0 / 48000.0)
-    # 2^24 sequential f32 adds; vectorised as a cumulative f32 sum in chunks.
-    acc = np.float32(0.0)
-    for _ in range(16):
-        chunk = np.full(1 << 20, step, np.float32)
-        chunk[0] = acc + step
-        acc = np.cumsum(chunk, dtype=np.float32)[-1]
-    exact = (1 << 24) * (44100.0 / 48000.0)
-    assert abs(float(acc) - exact) > 100.0
-
-
-def test_fixed_scale_truncates_and_saturates():  # fixed.rs:130-148
+def test_fixed_scale_truncates_and_saturates():  # Fixed::scale, fixed.rs:83-90
     s = O.lib().ko_fixed_scale
     assert s(1 << 32, 1 << 24) == 1 << 32
     assert s(3 << 32, (1 << 24) // 2) == (3 << 32) // 2
@@ -68,7 +58,7 @@ def test_fixed_scale_truncates_and_saturates():  # fixed.rs:130-148
     assert s(v, f) == (v * f) >> 24
 
 
-def test_bend_factor():  # fixed.rs:157-171
+def test_bend_factor():  # bend_factor, fixed.rs:101-113
     b = O.lib().ko_bend_factor
     assert b(0.0) == 1 << 24
     assert b(12.0) == 2 << 24
@@ -111,7 +101,7 @@ def test_pedal_defers_note_offs():  # voice.rs:690-710
     assert g.sounding() == 0
 
 
-def test_restrike_under_pedal():  # voice.rs:712-738
+def test_restrike_under_pedal():  # voice.rs:716-739
     g = _gates()
     s = H.GateTable.slot(0, 60)
     g.begin_block()
@@ -238,14 +228,14 @@ def test_resample_sine_keeps_its_frequency():  # resample.rs:124-145
     assert abs(freq - 1000.0) < 5.0
 
 
-def test_resample_upsampling_does_not_clip_headroom():  # resample.rs:147-160
+def test_resample_upsampling_does_not_clip_headroom():  # resample.rs:148-161
     t = np.arange(2000) / 44100.0
     src = np.trunc(26000.0 * np.sin(2.0 * np.pi * 440.0 * t)).astype(np.int16)
     out = H.resample_i16(src, 2.0)
     assert np.all(np.abs(out.astype(np.int32)) < 32000)
 
 
-def test_resample_extreme_input_saturates_instead_of_wrapping():  # resample.rs:162-170
+def test_resample_extreme_input_saturates_instead_of_wrapping():  # resample.rs:163-170
     src = np.where(np.arange(500) % 2 == 0, 32767, -32768).astype(np.int16)
     out = H.resample_i16(src, 2.0)
     assert out.dtype == np.int16 and out.size == 1000
