@@ -272,6 +272,7 @@ def run_cuda(args, world, rank, local):
     clk = clocks.stop()
     dt_ms = ev0.elapsed_time(ev1)
     passes, nblocks = B.timings_total()
+    ut, at = B.last_block_tiles()
     units = sum(n for _, n, *_ in dev[W:]) * bf
     # determinism: the replay must equal the host-buffer render byte for byte
     same = all(np.array_equal(e[5].cpu().numpy(), outs_a[i]) for i, e in enumerate(dev))
@@ -284,6 +285,7 @@ def run_cuda(args, world, rank, local):
         "same": same, "clocks": clk, "launches": launches, "preroll_s": t_pre, "preroll": preroll,
         "tiles": tiles, "bf": bf, "max_voices": cfg.max_voices, "sample_rate": cfg.sample_rate,
         "steal_percent": cfg.max_steal_percent, "stolen": B.stats().stolen, "dropped": B.stats().dropped,
+        "unit_share": ut / at if at else None,
     }
     B.close()
     A.close()
@@ -394,12 +396,17 @@ def run_served(args):
     bat = S.serve(jobs, mode=S.MODE_BATCHED, max_jobs=256, realtime_arrivals=not queued)
     clk = clocks.stop()
     seq = S.serve(jobs, mode=S.MODE_SEQUENTIAL, realtime_arrivals=not queued)
+    # The plain path on as many host threads as the batched server uses, one
+    # context and stream per job: many contexts at once, none batched.
+    par = S.serve(jobs, mode=S.MODE_PARALLEL, host_threads=int(bat.stats.host_threads),
+                  realtime_arrivals=not queued)
 
     def summary(r):
         lat = r.latencies()
         vs = r.stats.voice_samples
         return {"voice_samples_per_s": vs / r.stats.wall_s, "wall_s": r.stats.wall_s,
                 "gpu_s": r.stats.gpu_ms * 1e-3 if r.stats.gpu_ms else None,
+                "device_voice_samples_per_s": vs / (r.stats.gpu_ms * 1e-3) if r.stats.gpu_ms else None,
                 "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                 "mean_latency_s": float(lat.mean()), "steps": int(r.stats.steps),
                 "max_resident": int(r.stats.max_resident), "host_threads": int(r.stats.host_threads),
@@ -407,7 +414,8 @@ def run_served(args):
                 "failed_jobs": sum(1 for j in r.jobs if j.status != 0)}
 
     b, s = summary(bat), summary(seq)
-    same = bat.hashes() == seq.hashes()
+    p = summary(par)
+    same = bat.hashes() == seq.hashes() == par.hashes()
     audio_s = sum(j.blocks for j in bat.jobs) * 4096 / 48000
     blocks = sum(j.blocks for j in bat.jobs)
     line = {
@@ -422,8 +430,15 @@ def run_served(args):
                                f"each job bounded to its first {args.served_seconds:g} s of audio",
                    "jobs": len(jobs), "job_audio_s": audio_s, "job_blocks": blocks,
                    "arrivals": "queued" if queued else "poisson-realtime"},
-        "batched": b, "sequential_plain_path": s,
+        "batched": b, "sequential_plain_path": s, "parallel_plain_path": p,
         "ratio_vs_plain_path": b["voice_samples_per_s"] / s["voice_samples_per_s"],
+        "ratio_vs_parallel_plain_path": b["voice_samples_per_s"] / p["voice_samples_per_s"],
+        # Device time alone: the batch's launch sequences against the same
+        # jobs' blocks rendered one context at a time (each summed on the
+        # device with CUDA events), so host threads drop out of the ratio.
+        "device_ratio_vs_plain_path": (b["device_voice_samples_per_s"] / s["device_voice_samples_per_s"]
+                                       if b["device_voice_samples_per_s"] and s["device_voice_samples_per_s"]
+                                       else None),
         "p50_latency_s": b["p50_latency_s"], "p99_latency_s": b["p99_latency_s"],
         "outputs_identical_to_plain_path": same,
         "e2e": {"value": b["voice_samples_per_s"], "unit": "voice-samples/s", "h2d_bytes_per_step": None,
@@ -461,6 +476,78 @@ def workload_desc(name):
     }[name]
 
 
+# The reference arm renders the steal workloads at this fraction of their
+# pool and note count: the same per-voice work (durations, steal percent,
+# bank) at a size whose pre-roll to the steady state and timed blocks fit in
+# minutes on the host's cores.
+REFERENCE_SCALE = {"steal": 8, "steal-bent": 8}
+
+
+def bench_config(args, world):
+    """The workload the line is quoted on; both arms print this object."""
+    from kestrel_b200 import host as H
+    cfg, _, _ = H.config_workload(args.workload, seed=args.seed)
+    return {"workload": workload_desc(args.workload), "block_frames": cfg.block_frames,
+            "sample_rate": cfg.sample_rate, "max_voices": cfg.max_voices,
+            "mix": ["f32 tree", "two-sum", "f64"][args.mix_mode],
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (voice pool >= 1.8 GB at 8.4M voices)"
+                  if args.workload.startswith("steal") else "inputs smaller than L2 between blocks"}
+
+
+def run_reference(args, world):
+    """The reference arm: the CPU restatement of src/cpu.rs (the oracle) on
+    every host thread, on steady-state blocks of the workload. For the steal
+    workloads a bounded sample: the same workload at 1/REFERENCE_SCALE of its
+    pool and notes, pre-rolled on the oracle until its pool is saturated and
+    stealing, then W untimed and K timed blocks; one more block on a single
+    thread gives the reference's own (single-threaded) figure."""
+    from kestrel_b200 import host as H
+    from oracle.binding import OracleSynth
+    threads = os.cpu_count() or 1
+    cfg, bs, ms = H.config_workload(args.workload, seed=args.seed)
+    scale = REFERENCE_SCALE.get(args.workload, 1)
+    cfg.max_voices //= scale
+    ms.notes //= scale
+    cfg.mix_mode = args.mix_mode
+    bank = H.Bank(bs, cfg)
+    drv = H.Driver(cfg, bank, ms)
+    orc = OracleSynth(cfg, bank.pool, bank.params, threads=threads)
+    out = np.empty(cfg.block_frames * 2, np.float32)
+
+    def block():
+        live = orc.stats().active_voices
+        blk = drv.prepare(live)
+        t0 = time.perf_counter()
+        H.feed(orc, blk)
+        orc.render(out, keep_mix64=False)
+        dt = time.perf_counter() - t0
+        drv.finish(orc.stats().active_voices)
+        return live + len(blk.cmds), dt
+
+    t_pre = time.perf_counter()
+    pre, stealing = 0, 0
+    while pre < 160 and (pre < PREROLL.get(args.workload, 0) if scale == 1 else stealing < 2):
+        before = orc.stats().stolen
+        block()
+        pre += 1
+        stealing += orc.stats().stolen > before
+    t_pre = time.perf_counter() - t_pre
+    for _ in range(args.warmup):
+        block()
+    timed = [block() for _ in range(args.steps)]
+    orc.threads = 1
+    n1, t1 = block()
+    st = orc.stats()
+    orc.close()
+    secs = sum(dt for _, dt in timed)
+    units = sum(n for n, _ in timed) * cfg.block_frames
+    return {"value": units / secs if secs > 0 else 0.0, "secs": secs, "timed": timed, "threads": threads,
+            "single": n1 * cfg.block_frames / t1 if t1 > 0 else 0.0, "single_voices": n1, "preroll": pre,
+            "preroll_s": t_pre, "scale": scale, "max_voices": cfg.max_voices, "notes": ms.notes,
+            "stolen": st.stolen, "block_frames": cfg.block_frames, "sample_rate": cfg.sample_rate}
+
+
 def main(argv=None):
     args = parse_args(argv)
     world, rank, local = dist_env()
@@ -470,24 +557,29 @@ def main(argv=None):
     if args.impl == "reference":
         if rank != 0:
             return 0
-        threads = os.cpu_count() or 1
-        r = run_oracle(args.workload, args.seed, threads, args.warmup + args.steps, float("inf"))
-        # the first W blocks are warm-up
-        timed = r["per_block"][args.warmup:]
-        secs = sum(dt for _, dt in timed)
-        units = sum(n for n, _ in timed) * r["block_frames"]
-        value = units / secs if secs > 0 else 0.0
+        r = run_reference(args, world)
+        value, secs, K = r["value"], r["secs"], len(r["timed"])
+        mean_v = float(np.mean([n for n, _ in r["timed"]])) if K else 0.0
+        sample = (f"the workload at 1/{r['scale']} of its pool and notes ({r['max_voices']:,}-voice pool, "
+                  f"{r['notes']:,} notes, same durations, bank and steal percent), pre-rolled on the oracle for "
+                  f"{r['preroll']} blocks until saturated and stealing, then {args.warmup} untimed and {K} timed "
+                  f"steady-state blocks (mean {mean_v:,.0f} voices rendered per block)" if r["scale"] > 1 else
+                  f"blocks {r['preroll'] + args.warmup}..{r['preroll'] + args.warmup + K - 1} of the workload after "
+                  f"a {r['preroll']}-block pre-roll (mean {mean_v:,.0f} voices per block)")
         line = {
             "metric": metric, "value": value, "unit": unit, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(len(timed), 1),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(K, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "x_realtime": (len(timed) * r["block_frames"] / r["sample_rate"]) / secs if secs > 0 else 0.0,
-            "config": {"workload": workload_desc(args.workload), "steps_are": "the workload's first blocks",
-                       "live_voices_max": r["live_max"]},
-            "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
-                             "sample": f"blocks {args.warmup}..{args.warmup + len(timed) - 1} of the workload "
-                                       f"(up to {r['live_max']} voices), C++ restatement of src/cpu.rs, "
-                                       f"voice loop split over {threads} threads"},
+            "x_realtime": (K * r["block_frames"] / r["sample_rate"]) / secs if secs > 0 else 0.0,
+            "config": bench_config(args, world),
+            "cpu_baseline": {"value": value, "unit": unit, "cores": r["threads"], "kind": "port",
+                             "sample": sample + f"; C++ restatement of src/cpu.rs, voice loop split over "
+                                                f"{r['threads']} threads"},
+            # The reference backend is single-threaded (README.md:113-117):
+            # the next steady-state block on one thread.
+            "single_thread": {"value": r["single"], "unit": unit, "cores": 1,
+                              "voices_rendered": r["single_voices"]},
+            "preroll_s": r["preroll_s"], "stolen": r["stolen"],
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line), flush=True)
@@ -531,13 +623,10 @@ def main(argv=None):
             "warmup": args.warmup, "ms_per_step": ms_t / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "x_realtime": (K * r["bf"] / r["sample_rate"]) / (ms_t * 1e-3),
-            "config": {"workload": workload_desc(args.workload), "block_frames": r["bf"],
-                       "sample_rate": r["sample_rate"], "max_voices": r["max_voices"],
-                       "mean_voices_rendered": round(n_render_mean), "preroll_blocks": r["preroll"],
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (voice pool >= 1.8 GB at 8.4M voices)"
-                             if args.workload.startswith("steal") else "inputs smaller than L2 between blocks",
-                       "replay_equals_host_render": r["same"]},
+            "config": bench_config(args, world),
+            "measured": {"mean_voices_rendered": round(n_render_mean), "preroll_blocks": r["preroll"],
+                         "replay_equals_host_render": r["same"], "stolen": r["stolen"],
+                         "unit_path_share": r["unit_share"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_render",
                          "algorithmic_bytes_per_launch": bytes_launch,

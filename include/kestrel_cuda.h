@@ -363,6 +363,10 @@ int kc_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
  * plus the admitted commands (the per-block term of the voice-samples
  * metric). */
 int kc_last_block_voices(kc_synth* s, uint32_t* rendered);
+/* How the last completed block's render ran: 16-frame warp-tiles classified
+ * onto the unit-step or integral-step path, and all warp-tiles. No
+ * counterpart in the reference; a measure of the workload's pitch mix. */
+int kc_last_block_tiles(kc_synth* s, uint32_t* unit_tiles, uint32_t* all_tiles);
 
 /* ---- inspection (tests) ------------------------------------------------- *
  * Copies the live part of the voice pool to the host as 24 SoA fields of

@@ -18,6 +18,11 @@
  *   KS_MODE_SEQUENTIAL  the plain path: one job at a time in arrival order,
  *                       each block through kc_render on one thread, as a user
  *                       of the reference renders files one after another.
+ *   KS_MODE_PARALLEL    the plain path on host_threads threads at once: each
+ *                       thread takes the next job in arrival order and
+ *                       renders it to completion through kc_render on its own
+ *                       context and stream, admitted by the same VRAM budget.
+ *                       Many contexts share the device, none batched.
  *
  * Results report each job's arrival, admission, first block and completion on
  * the server clock, its voice-samples, and a 64-bit hash of its output bytes:
@@ -39,6 +44,7 @@ extern "C" {
 
 #define KS_MODE_BATCHED 0u
 #define KS_MODE_SEQUENTIAL 1u
+#define KS_MODE_PARALLEL 2u
 
 typedef struct ks_job_spec {
     double arrival_s;            /* seconds after the server starts */
@@ -90,7 +96,9 @@ typedef struct ks_job_result {
 
 typedef struct ks_run_stats {
     double wall_s;               /* server start to the last completion */
-    double gpu_ms;               /* device time of the render launch sequences */
+    double gpu_ms;               /* device time of the render launch sequences: summed over batch
+                                    steps (batched) or over every job's blocks (sequential,
+                                    parallel; in parallel mode the jobs' blocks overlap) */
     double setup_s;              /* host time spent on banks and drivers, summed */
     uint64_t voice_samples;
     uint64_t job_blocks;

@@ -195,6 +195,12 @@ class CudaSynth:
         N.check(self._lib.kc_last_block_voices(self._h, C.byref(n)), self._lib)
         return n.value
 
+    def last_block_tiles(self) -> tuple[int, int]:
+        """(unit- or integral-step warp-tiles, all warp-tiles) of the last block."""
+        u, a = C.c_uint32(), C.c_uint32()
+        N.check(self._lib.kc_last_block_tiles(self._h, C.byref(u), C.byref(a)), self._lib)
+        return u.value, a.value
+
 
 class CudaBatch:
     """One block of many contexts per call (kc_batch_render).

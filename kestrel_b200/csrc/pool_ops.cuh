@@ -358,9 +358,12 @@ constexpr uint32_t SORT_RADIX_MIN = 4, SORT_RADIX_MAX = 10, SORT_RADIX_DEFAULT =
 
 // Pass `shift`: count digit occurrences per CTA chunk into counts[d * G + cta].
 // Pass 0 computes keys from the pool; later passes read the key array.
+// `totals` (when given) also receives each digit's count over all CTAs, for
+// sort_offsets_body; it must be zero when the pass starts.
 template <uint32_t RB>
 __device__ __forceinline__ void sort_count_body(PoolArgs a, SortLayout L, const uint32_t* keys, uint32_t shift,
-                                                uint32_t* counts, uint32_t cta, uint32_t ctas) {
+                                                uint32_t* counts, uint32_t cta, uint32_t ctas,
+                                                uint32_t* totals = nullptr) {
     constexpr uint32_t BINS = 1u << RB;
     __shared__ uint32_t h[BINS];
     const uint32_t n = a.st->live_render;
@@ -373,7 +376,44 @@ __device__ __forceinline__ void sort_count_body(PoolArgs a, SortLayout L, const 
         atomicAdd(&h[(k >> shift) & (BINS - 1u)], 1u);
     }
     __syncthreads();
-    for (uint32_t d = threadIdx.x; d < BINS; d += blockDim.x) counts[d * ctas + cta] = h[d];
+    for (uint32_t d = threadIdx.x; d < BINS; d += blockDim.x) {
+        counts[d * ctas + cta] = h[d];
+        if (totals && h[d]) atomicAdd(&totals[d], h[d]);
+    }
+}
+
+// The digit-major exclusive scan of counts[d * ctas + c] for one pass, one
+// warp per digit d (any number of CTAs of any width): the digit's base is the
+// sum of the totals of the digits below it, and the warp scans its digit's
+// per-CTA counts in place on top of that base (each lane a contiguous run of
+// CTAs, lane sums scanned with shuffles). The last digit writes the grand
+// total. Replaces a single-CTA scan of all 2^RB * ctas words.
+__device__ __forceinline__ void sort_offsets_body(uint32_t* counts, uint32_t ctas, uint32_t bins,
+                                                  const uint32_t* totals, uint32_t* total, uint32_t d) {
+    if (d >= bins) return;
+    const uint32_t lane = lane_id();
+    uint32_t base = 0;
+    for (uint32_t k = lane; k < d; k += 32u) base += totals[k];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) base += __shfl_xor_sync(0xFFFFFFFFu, base, o);
+    uint32_t* row = counts + (size_t)d * ctas;
+    const uint32_t per = (ctas + 31u) / 32u;
+    const uint32_t c0 = min(ctas, lane * per), c1 = min(ctas, c0 + per);
+    uint32_t local = 0;
+    for (uint32_t c = c0; c < c1; ++c) local += row[c];
+    uint32_t x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    uint32_t run = base + x - local;
+    for (uint32_t c = c0; c < c1; ++c) {
+        const uint32_t v = row[c];
+        row[c] = run;
+        run += v;
+    }
+    if (d == bins - 1u && lane == 31u) *total = run;
 }
 
 // Stable scatter of one pass. keys_in == nullptr on the first pass (keys and

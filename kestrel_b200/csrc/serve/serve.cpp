@@ -246,6 +246,18 @@ int finish(Job& j, const ks_server_config& sc, double now) {
     return KC_OK;
 }
 
+// Device milliseconds of every block a job's context rendered (its per-pass
+// event timings, switched on when the context was created).
+double device_ms(Job& j) {
+    if (!j.synth) return 0.0;
+    double ms[8] = {};  // kc_timings_total fills one entry per pass (five)
+    uint64_t blocks = 0;
+    if (kc_timings_total(j.synth, ms, 8, &blocks)) return 0.0;
+    double t = 0.0;
+    for (double x : ms) t += x;
+    return t;
+}
+
 bool same_batch_variant(const kc_config& a, const kc_config& b) {
     const uint32_t va = a.voices_per_lane == 2 ? 2 : 1, vb = b.voices_per_lane == 2 ? 2 : 1;
     const uint32_t ra = a.sort_radix_bits ? a.sort_radix_bits : 8, rb = b.sort_radix_bits ? b.sort_radix_bits : 8;
@@ -263,7 +275,7 @@ int serve_sequential(const ks_server_config& sc, std::vector<Job>& jobs, const s
         }
         setup(j);
         rs.setup_s += j.res->setup_s;
-        if (j.status == KC_OK) create(j);
+        if (j.status == KC_OK && create(j) == KC_OK) kc_set_profile(j.synth, 1);
         j.res->admit_s = since(t0);
         rs.max_resident = 1;
         rs.peak_device_bytes = std::max(rs.peak_device_bytes, j.res->device_bytes);
@@ -286,11 +298,108 @@ int serve_sequential(const ks_server_config& sc, std::vector<Job>& jobs, const s
         }
         j.res->done_s = since(t0);
         j.res->status = j.status;
+        rs.gpu_ms += device_ms(j);
         if (trace_on())
             std::fprintf(stderr, "[serve] t=%.3f job=%u blocks=%llu setup_s=%.3f run_s=%.3f status=%d\n", since(t0), j.id,
                          (unsigned long long)j.res->blocks, j.res->setup_s, j.res->done_s - j.res->admit_s, j.status);
         release(j);
     }
+    return KC_OK;
+}
+
+// The plain path on several host threads at once: each thread takes the next
+// job in arrival order, builds its bank and driver, waits until the job's
+// device-byte bound fits the budget beside the jobs already running, and
+// renders it to completion through kc_render on its own context (and so its
+// own stream). Jobs run side by side on the device, one context each, with
+// no batching: the baseline that shows what batching adds beyond running
+// many contexts at once.
+int serve_parallel(const ks_server_config& sc, std::vector<Job>& jobs, const std::vector<uint32_t>& order,
+                   ks_run_stats& rs, Clock::time_point t0) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned n_threads = std::min<unsigned>(sc.host_threads ? sc.host_threads : hw, (unsigned)jobs.size());
+    rs.host_threads = n_threads;
+    uint64_t budget = sc.vram_budget;
+    if (!budget) {
+        uint64_t f = 0, t = 0;
+        if (int rc = kc_device_memory((int)sc.device, &f, &t)) return fail(rc, kc_last_error());
+        const uint64_t reserve = 8ull << 30;
+        budget = f > reserve ? f - reserve : f / 2;
+    }
+    std::mutex m;
+    std::condition_variable cv;
+    size_t next = 0;
+    uint64_t used = 0;
+    uint32_t running = 0;
+    auto worker = [&] {
+        for (;;) {
+            uint32_t id;
+            {
+                std::lock_guard<std::mutex> g(m);
+                if (next >= order.size()) return;
+                id = order[next++];
+            }
+            Job& j = jobs[id];
+            if (sc.realtime_arrivals) {
+                const double wait = j.spec->arrival_s - since(t0);
+                if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
+            }
+            setup(j);
+            {
+                std::unique_lock<std::mutex> g(m);
+                rs.setup_s += j.res->setup_s;
+                if (j.status == KC_OK && j.est_bytes > budget) {
+                    j.status = KC_ERR_OOM;
+                    j.err = "job needs more device memory than the budget";
+                }
+                if (j.status == KC_OK) {
+                    cv.wait(g, [&] { return running == 0 || used + j.est_bytes <= budget; });
+                    used += j.est_bytes;
+                    ++running;
+                    rs.max_resident = std::max(rs.max_resident, running);
+                    rs.peak_device_bytes = std::max(rs.peak_device_bytes, used);
+                }
+            }
+            const bool admitted = j.status == KC_OK;
+            if (admitted && create(j) == KC_OK) kc_set_profile(j.synth, 1);
+            j.res->admit_s = since(t0);
+            uint64_t blocks = 0;
+            while (j.status == KC_OK && !j.finished) {
+                if (int rc = prepare(j)) {
+                    j.status = rc;
+                    j.err = g_err;
+                    break;
+                }
+                if (int rc = kc_render(j.synth, j.out.data(), j.out.size())) {
+                    j.status = rc;
+                    j.err = kc_last_error();
+                    break;
+                }
+                if (int rc = finish(j, sc, since(t0))) {
+                    j.status = rc;
+                    j.err = g_err;
+                }
+                ++blocks;
+            }
+            j.res->done_s = since(t0);
+            j.res->status = j.status;
+            const double ms = device_ms(j);
+            release(j);
+            {
+                std::lock_guard<std::mutex> g(m);
+                rs.gpu_ms += ms;
+                rs.steps += blocks;
+                if (admitted) {
+                    used -= std::min(used, j.est_bytes);
+                    --running;
+                }
+            }
+            cv.notify_all();
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned i = 0; i < n_threads; ++i) th.emplace_back(worker);
+    for (auto& t : th) t.join();
     return KC_OK;
 }
 
@@ -684,7 +793,7 @@ uint64_t ks_hash_block(uint64_t h, const float* out, size_t n) {
 int ks_serve(const ks_server_config* cfg, const ks_job_spec* specs, uint32_t n_jobs, ks_job_result* results,
              ks_run_stats* stats) {
     if (!cfg || (n_jobs && (!specs || !results)) || !stats) return fail(KC_ERR_INVALID, "null argument");
-    if (cfg->mode > KS_MODE_SEQUENTIAL) return fail(KC_ERR_INVALID, "unknown server mode");
+    if (cfg->mode > KS_MODE_PARALLEL) return fail(KC_ERR_INVALID, "unknown server mode");
     if (cfg->max_jobs == 0 || cfg->max_jobs > 1024) return fail(KC_ERR_INVALID, "max_jobs must be in 1..=1024");
     std::memset(stats, 0, sizeof(*stats));
     if (n_jobs == 0) return KC_OK;
@@ -734,6 +843,7 @@ int ks_serve(const ks_server_config* cfg, const ks_job_spec* specs, uint32_t n_j
     if (cfg->device_resample) kh_set_resampler(kc_resample_i16_batch, &resample_device);
     const auto t0 = Clock::now();
     const int rc = cfg->mode == KS_MODE_SEQUENTIAL ? serve_sequential(*cfg, jobs, order, *stats, t0)
+                   : cfg->mode == KS_MODE_PARALLEL ? serve_parallel(*cfg, jobs, order, *stats, t0)
                                                    : serve_batched(*cfg, jobs, order, *stats, t0);
     if (cfg->device_resample) kh_set_resampler(nullptr, nullptr);
     stats->wall_s = since(t0);

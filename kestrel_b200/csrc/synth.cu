@@ -55,39 +55,52 @@ __global__ void k_commit(DevState* st, const uint32_t* total) { commit_body(st, 
 
 template <uint32_t RB>
 __global__ void __launch_bounds__(256) k_sort_count(PoolArgs a, SortLayout L, const uint32_t* keys,
-                                                    uint32_t shift, uint32_t* counts) {
-    sort_count_body<RB>(a, L, keys, shift, counts, blockIdx.x, gridDim.x);
+                                                    uint32_t shift, uint32_t* counts, uint32_t* totals) {
+    sort_count_body<RB>(a, L, keys, shift, counts, blockIdx.x, gridDim.x, totals);
 }
 
+// One warp per digit: 8 digits per CTA.
+__global__ void __launch_bounds__(256) k_sort_offsets(uint32_t* counts, uint32_t ctas, uint32_t bins,
+                                                      const uint32_t* totals, uint32_t* total) {
+    sort_offsets_body(counts, ctas, bins, totals, total, blockIdx.x * 8u + (threadIdx.x >> 5));
+}
+
+// The scatter also clears the digit totals for the next pass (nothing reads
+// them once the offsets are formed).
 template <uint32_t RB>
 __global__ void __launch_bounds__(256) k_sort_scatter(PoolArgs a, SortLayout L, const uint32_t* keys_in,
                                                       const uint32_t* idx_in, uint32_t* keys_out,
                                                       uint32_t* idx_out, uint32_t shift,
-                                                      const uint32_t* offsets) {
+                                                      const uint32_t* offsets, uint32_t* totals) {
+    if (blockIdx.x == 0)
+        for (uint32_t d = threadIdx.x; d < (1u << RB); d += blockDim.x) totals[d] = 0u;
     sort_scatter_body<RB>(a, L, keys_in, idx_in, keys_out, idx_out, shift, offsets, blockIdx.x, gridDim.x);
 }
 
-// One LSD pass of the pool sort at digit width RB: count, scan, scatter.
+// One LSD pass of the pool sort at digit width RB: count (with the digit
+// totals), the digit-major offsets, scatter. `totals` is zero on entry and on
+// return.
 template <uint32_t RB>
 void sort_pass(cudaStream_t q, uint32_t G, const PoolArgs& pa, const SortLayout& L, const uint32_t* kin,
                const uint32_t* iin, uint32_t* kout, uint32_t* iout, uint32_t shift, uint32_t* counts,
-               uint32_t* total) {
-    k_sort_count<RB><<<G, 256, 0, q>>>(pa, L, kin, shift, counts);
-    k_scan_counts<<<1, 1024, 0, q>>>(counts, (1u << RB) * G, total);
-    k_sort_scatter<RB><<<G, 256, 0, q>>>(pa, L, kin, iin, kout, iout, shift, counts);
+               uint32_t* totals, uint32_t* total) {
+    constexpr uint32_t BINS = 1u << RB;
+    k_sort_count<RB><<<G, 256, 0, q>>>(pa, L, kin, shift, counts, totals);
+    k_sort_offsets<<<(BINS + 7u) / 8u, 256, 0, q>>>(counts, G, BINS, totals, total);
+    k_sort_scatter<RB><<<G, 256, 0, q>>>(pa, L, kin, iin, kout, iout, shift, counts, totals);
 }
 
 void sort_pass_rb(uint32_t rb, cudaStream_t q, uint32_t G, const PoolArgs& pa, const SortLayout& L,
                   const uint32_t* kin, const uint32_t* iin, uint32_t* kout, uint32_t* iout, uint32_t shift,
-                  uint32_t* counts, uint32_t* total) {
+                  uint32_t* counts, uint32_t* totals, uint32_t* total) {
     switch (rb) {
-        case 4: sort_pass<4>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
-        case 5: sort_pass<5>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
-        case 6: sort_pass<6>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
-        case 7: sort_pass<7>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
-        case 9: sort_pass<9>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
-        case 10: sort_pass<10>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
-        default: sort_pass<8>(q, G, pa, L, kin, iin, kout, iout, shift, counts, total); break;
+        case 4: sort_pass<4>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        case 5: sort_pass<5>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        case 6: sort_pass<6>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        case 7: sort_pass<7>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        case 9: sort_pass<9>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        case 10: sort_pass<10>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        default: sort_pass<8>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
     }
 }
 
@@ -238,6 +251,7 @@ void free_all(kc_synth* s) {
     cudaFree(s->sel_hist);
     cudaFree(s->counts);
     cudaFree(s->total);
+    cudaFree(s->sort_totals);
     for (int i = 0; i < 2; ++i) {
         cudaFree(s->keys[i]);
         cudaFree(s->idx[i]);
@@ -378,7 +392,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
             const uint32_t* kin = p == 0 ? nullptr : s->keys[cur];
             const uint32_t* iin = p == 0 ? nullptr : s->idx[cur];
             sort_pass_rb(s->radix, q, G, pa, s->sort, kin, iin, s->keys[cur ^ 1], s->idx[cur ^ 1], shift, s->counts,
-                         s->total + 1);
+                         s->sort_totals, s->total + 1);
             cur ^= 1;
         }
         k_sort_gather<<<s->pool_ctas, 256, 0, q>>>(pa, s->idx[cur]);
@@ -430,6 +444,7 @@ uint64_t footprint(const kc_config& c, uint64_t cap, uint64_t pcm_len, uint64_t 
     if (c.mix_mode == KC_MIX_TWO_SUM) n += (uint64_t)partial_slices * samples * 4;
     n += sizeof(DevState) + sizeof(BlockCtl) + SEL_ROUNDS * 256 * 4 + 16;
     n += (uint64_t)std::max<uint32_t>(256u, 1u << radix_of(c)) * compact_ctas * 4;  // digit counts
+    n += (1u << SORT_RADIX_MAX) * 4;                                            // digit totals
     if (c.sort_voices) n += 4ull * cap * 4;                                     // keys, indices
     return n;
 }
@@ -584,6 +599,8 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaMalloc(&s->sel_hist, SEL_ROUNDS * 256 * 4));
     KC_TRY(cudaMalloc(&s->counts, (size_t)std::max<uint32_t>(256u, 1u << s->radix) * s->compact_ctas * 4));
     KC_TRY(cudaMalloc(&s->total, 16));
+    KC_TRY(cudaMalloc(&s->sort_totals, (1u << SORT_RADIX_MAX) * 4));
+    KC_TRY(cudaMemset(s->sort_totals, 0, (1u << SORT_RADIX_MAX) * 4));
     if (cfg->sort_voices) {
         for (int i = 0; i < 2; ++i) {
             KC_TRY(cudaMalloc(&s->keys[i], (size_t)s->cap * 4));
@@ -882,6 +899,13 @@ int kc_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes) {
 int kc_last_block_voices(kc_synth* s, uint32_t* rendered) {
     if (!s || !rendered) return fail(KC_ERR_INVALID, "null argument");
     *rendered = s->h_st->live_render;
+    return KC_OK;
+}
+
+int kc_last_block_tiles(kc_synth* s, uint32_t* unit_tiles, uint32_t* all_tiles) {
+    if (!s || !unit_tiles || !all_tiles) return fail(KC_ERR_INVALID, "null argument");
+    *unit_tiles = s->h_st->unit_tiles;
+    *all_tiles = s->h_st->all_tiles;
     return KC_OK;
 }
 

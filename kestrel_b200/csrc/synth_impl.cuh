@@ -47,6 +47,7 @@ struct kc_synth {
     uint32_t* sel_hist = nullptr;
     uint32_t* counts = nullptr;
     uint32_t* total = nullptr;
+    uint32_t* sort_totals = nullptr;  // per-digit totals of the pool-sort pass in flight (zero between passes)
     uint32_t* keys[2] = {nullptr, nullptr};
     uint32_t* idx[2] = {nullptr, nullptr};
 

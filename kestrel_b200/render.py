@@ -258,7 +258,7 @@ def main(argv=None) -> int:
                     help="SoundFont 2 file (default: the workload's synthetic bank)")
     ap.add_argument("-o", "--out", default=None, help="output WAV")
     ap.add_argument("--midi", dest="midi_opt", default=None, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["plain", "black", "steal"], default="plain")
+    ap.add_argument("--workload", choices=["plain", "black", "steal", "steal-bent"], default="plain")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--write-sf2", default=None, help="write the workload's synthetic bank as a .sf2 file and exit")
     ap.add_argument("--write-midi", default=None, help="write the workload's synthetic stream as a .mid file and exit")

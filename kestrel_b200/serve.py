@@ -22,7 +22,7 @@ from . import native as N
 
 SERVE_LIB_PATH = Path(__file__).resolve().parent / "libkestrel_serve.so"
 
-MODE_BATCHED, MODE_SEQUENTIAL = 0, 1
+MODE_BATCHED, MODE_SEQUENTIAL, MODE_PARALLEL = 0, 1, 2
 
 
 class KsJobSpec(C.Structure):

@@ -109,6 +109,12 @@ def test_batched_equals_sequential_equals_alone():
     assert [r.voice_samples for r in seq.jobs] == [r.voice_samples for r in bat.jobs]
     assert 2 <= bat.stats.max_resident <= 3     # jobs overlapped on the device, never more than the slots
     assert seq.stats.max_resident == 1
+    assert seq.stats.gpu_ms > 0 and bat.stats.gpu_ms > 0   # device time recorded in both modes
+    # the plain path on four threads at once, one context per job
+    par = S.serve(jobs, mode=S.MODE_PARALLEL, host_threads=4, realtime_arrivals=False)
+    assert all(r.status == 0 for r in par.jobs)
+    assert par.hashes() == seq.hashes()
+    assert 2 <= par.stats.max_resident <= 4 and par.stats.host_threads == 4
     for k in (0, 3):
         assert _alone(jobs[k]) == seq.jobs[k].out_hash
     # arrivals on the wall clock: each job is admitted no earlier than it arrives
