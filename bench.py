@@ -285,7 +285,7 @@ def run_cuda(args, world, rank, local):
         "same": same, "clocks": clk, "launches": launches, "preroll_s": t_pre, "preroll": preroll,
         "tiles": tiles, "bf": bf, "max_voices": cfg.max_voices, "sample_rate": cfg.sample_rate,
         "steal_percent": cfg.max_steal_percent, "stolen": B.stats().stolen, "dropped": B.stats().dropped,
-        "unit_share": ut / at if at else None,
+        "hot_share": ut / at if at else None,
     }
     B.close()
     A.close()
@@ -626,7 +626,7 @@ def main(argv=None):
             "config": bench_config(args, world),
             "measured": {"mean_voices_rendered": round(n_render_mean), "preroll_blocks": r["preroll"],
                          "replay_equals_host_render": r["same"], "stolen": r["stolen"],
-                         "unit_path_share": r["unit_share"]},
+                         "hot_path_share": r["hot_share"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_render",
                          "algorithmic_bytes_per_launch": bytes_launch,

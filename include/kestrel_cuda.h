@@ -144,10 +144,11 @@ typedef struct kc_config {
     uint32_t voices_per_lane;    /* render voices per GPU lane: 0 = default (1), 1 or 2 */
     uint32_t sort_radix_bits;    /* key bits per pool-sort pass, 4..=10; 0 = default (8). The
                                     sorted order is the same for every width. */
-    uint32_t unit_tile_frames;   /* frames per render tile on the unit and integral-step paths
-                                    (one voice per lane, f32 tree mix): 16, 32, or 0 = chosen
-                                    per block (32 when the block before ran mostly on those
-                                    paths). The output is the same for every choice. */
+    uint32_t unit_tile_frames;   /* frames per render tile on the hot paths -- unit, integral
+                                    and fractional steps with no envelope transition (one voice
+                                    per lane, f32 tree mix): 16, 32, or 0 = chosen per block (32
+                                    when the block before ran mostly on those paths). The
+                                    output is the same for every choice. */
     uint32_t reserved[4];
 } kc_config;
 
@@ -364,9 +365,10 @@ int kc_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes);
  * metric). */
 int kc_last_block_voices(kc_synth* s, uint32_t* rendered);
 /* How the last completed block's render ran: 16-frame warp-tiles classified
- * onto the unit-step or integral-step path, and all warp-tiles. No
- * counterpart in the reference; a measure of the workload's pitch mix. */
-int kc_last_block_tiles(kc_synth* s, uint32_t* unit_tiles, uint32_t* all_tiles);
+ * onto a hot path (every lane live and sounding with no envelope transition:
+ * unit, integral or fractional step), and all warp-tiles. No counterpart in
+ * the reference; the render picks 32-frame hot tiles when most tiles are. */
+int kc_last_block_tiles(kc_synth* s, uint32_t* hot_tiles, uint32_t* all_tiles);
 
 /* ---- inspection (tests) ------------------------------------------------- *
  * Copies the live part of the voice pool to the host as 24 SoA fields of

@@ -196,7 +196,8 @@ class CudaSynth:
         return n.value
 
     def last_block_tiles(self) -> tuple[int, int]:
-        """(unit- or integral-step warp-tiles, all warp-tiles) of the last block."""
+        """(hot-path warp-tiles -- unit, integral or fractional step -- and all
+        warp-tiles) of the last block."""
         u, a = C.c_uint32(), C.c_uint32()
         N.check(self._lib.kc_last_block_tiles(self._h, C.byref(u), C.byref(a)), self._lib)
         return u.value, a.value

@@ -418,7 +418,7 @@ struct kc_batch {
     uint32_t radix = 8;
     void* render_fn = nullptr;
     void* render_fn2 = nullptr;    // 32-frame unit tiles (null where not built)
-    bool unit_tiles = false;       // the last batch ran mostly on unit spans
+    bool hot_tiles = false;       // the last batch ran mostly on hot tiles
     size_t render_smem = 0;
     uint32_t render_ctas = 0;
     uint32_t pass_ctas = 0;
@@ -726,7 +726,7 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
     KB_CUDA(cudaEventRecord(b->ev0, q));
     // Both tile lengths leave the same bits; the last batch's unit-path
     // share picks the faster one.
-    const bool dbl = b->unit_tiles && b->render_fn2;
+    const bool dbl = b->hot_tiles && b->render_fn2;
     if (b->exec && (!dbl || b->exec2)) KB_CUDA(cudaGraphLaunch(dbl ? b->exec2 : b->exec, q));
     else if (int rc = enqueue_passes(b, dbl ? b->render_fn2 : b->render_fn)) return rc;
     KB_CUDA(cudaEventRecord(b->ev1, q));
@@ -750,13 +750,13 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         s->stats.stolen = st.stolen;
         s->stats.dropped = st.dropped;
         std::memcpy(&s->stats.peak, &st.peak_bits, 4);
-        unit += st.unit_tiles;
+        unit += st.hot_tiles;
         all += st.all_tiles;
-        if (st.all_tiles) s->unit_tiles = (uint64_t)st.unit_tiles * 2u >= st.all_tiles;
+        if (st.all_tiles) s->hot_tiles = (uint64_t)st.hot_tiles * 2u >= st.all_tiles;
         if (st.error && rc == KC_OK)
             rc = fail(KC_ERR_DEVICE, "job " + std::to_string(j) + ": device error word " + std::to_string(st.error));
     }
-    if (all) b->unit_tiles = unit * 2u >= all;
+    if (all) b->hot_tiles = unit * 2u >= all;
     return rc;
 }
 

@@ -83,7 +83,7 @@ struct DevState {
     uint64_t dropped;      // cumulative
     uint32_t peak_bits;    // max |out| of the block, as f32 bits
     uint32_t active_warps; // render warps that own at least one voice
-    uint32_t unit_tiles;   // warp-tiles the render ran on the unit or integral-step path
+    uint32_t hot_tiles;    // warp-tiles the render ran on a hot path (unit, integral or fractional step)
     uint32_t all_tiles;    // warp-tiles the render ran
     uint32_t pad[2];
 };

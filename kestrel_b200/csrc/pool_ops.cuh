@@ -58,7 +58,7 @@ __device__ __forceinline__ void admit_state(PoolArgs a, BlockCtl* ctl, uint32_t 
     st->sel_prefix = 0;
     st->sel_k = (uint32_t)need;
     st->peak_bits = 0;
-    st->unit_tiles = 0;
+    st->hot_tiles = 0;
     st->all_tiles = 0;
     // Must match k_render's batching: 32 * voices-per-lane voices per warp.
     const uint64_t n = live + take;

@@ -690,6 +690,8 @@ struct Taps<false> {
 //  P_HOT   fractional phases: two taps and the lerp, the 32.32 phase per frame.
 // fast_ok proved every tap in bounds and phase + 16 * step free of overflow,
 // so P_UNIT and P_INT write the phase back once at the end of the tile.
+// Each tile also prefetches into L1 the line its lane reads next (the tile
+// after this one), so the next tile's first taps do not wait on L2.
 template <int KIND, int FM, bool STRICT, bool F32, int V, bool FACTOR, uint32_t NT = MIX_TILE>
 __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a, const EnvStep (&e)[V], float* sm,
                                          uint32_t lane) {
@@ -699,6 +701,15 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
         Taps<F32> t[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) t[k] = Taps<F32>(a, v[k].base + (uint32_t)(v[k].phase >> 32));
+        if constexpr (F32) {
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                // The last tap of the next tile's line, clamped into the f32
+                // pool and its zero pad (a neutral lane sits at the pad).
+                const uint32_t nx = min(v[k].base + (uint32_t)(v[k].phase >> 32) + NT + 31u, a.pcm_len + 31u);
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(a.pcmf + nx));
+            }
+        }
 #pragma unroll
         for (uint32_t i = 0; i < NT; ++i) {
             float y[V];
@@ -741,7 +752,15 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
         // five and one load instead of two.
         uint64_t q[V];
 #pragma unroll
-        for (int k = 0; k < V; ++k) q[k] = v[k].phase + ((uint64_t)v[k].base << 32);
+        for (int k = 0; k < V; ++k) {
+            q[k] = v[k].phase + ((uint64_t)v[k].base << 32);
+            // The next tile's first pair and the line after it: fast_ok
+            // bounded the span's last index below pcm_len, and the table runs
+            // ZERO_PAD entries past it.
+            const float2* nx = a.pcmp + (uint32_t)((q[k] + (v[k].step << LOG_NT)) >> 32);
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(nx));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(nx + 16));
+        }
 #pragma unroll
         for (uint32_t i = 0; i < NT; ++i) {
             float y[V];
@@ -783,7 +802,7 @@ __device__ __forceinline__ void hot_dispatch(int path, VoiceRegs (&v)[V], const 
                                              float* sm, uint32_t lane) {
     if (path == P_UNIT) hot_tile<P_UNIT, FM, STRICT, F32, V, FACTOR, NT>(v, a, e, sm, lane);
     else if (path == P_INT) hot_tile<P_INT, FM, STRICT, F32, V, FACTOR, NT>(v, a, e, sm, lane);
-    else if constexpr (INTERP == KC_INTERP_LINEAR && NT == MIX_TILE)
+    else if constexpr (INTERP == KC_INTERP_LINEAR)
         hot_tile<P_HOT, FM, STRICT, F32, V, FACTOR, NT>(v, a, e, sm, lane);
 }
 
@@ -804,7 +823,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
     const uint32_t lane = lane_id();
     constexpr bool FACTOR = V == 1 && MIX == KC_MIX_F32_TREE;
     static_assert(!DOUBLE || FACTOR, "32-frame tiles are factored ones");
-    uint32_t unit_tiles = 0;  // tiles classified onto the unit or integral-step path
+    uint32_t hot_tiles = 0;   // tiles classified onto a hot path (unit, integral or fractional step)
     const uint32_t per = 32u * V;
     const uint32_t nbatch = (n + per - 1u) / per;
     const uint32_t samples = a.block_frames * 2u;
@@ -876,15 +895,14 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 }
                 if (!carry_left) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e, fm);
                 carried = path;
-                if (path <= P_INT) unit_tiles += carry_left + 1u;
+                if (path <= P_HOT) hot_tiles += carry_left + 1u;
             }
-            // A unit or integral-step tile whose successor is in the same
-            // span and behind no gate row runs with it as one 32-frame tile.
-            // (Fractional-step tiles stay 16 frames: doubling them measured
-            // slower.)
+            // A hot tile (unit, integral or fractional step) whose successor
+            // is in the same span and behind no gate row runs with it as one
+            // 32-frame tile.
             nt = MIX_TILE;
             float part_prev2 = 0.0f;
-            if (DOUBLE && path <= P_INT && carry_left && f0 + MIX_TILE != next_gate) {
+            if (DOUBLE && path <= P_HOT && carry_left && f0 + MIX_TILE != next_gate) {
                 nt = 2u * MIX_TILE;
                 --carry_left;
                 if (!first) part_prev2 = part[j + 2u * MIX_TILE];
@@ -1071,12 +1089,11 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
             if (vi < n) store_voice(v[k], a, vi);
         }
     }
-    // How much of the block ran on the unit or integral-step path: the host
-    // picks the next block's tile length by it (the output is the same
-    // either way).
+    // How much of the block ran on the hot paths: the host picks the next
+    // block's tile length by it (the output is the same either way).
     if (lane == 0 && gw < nbatch) {
         const uint32_t mine = (nbatch - gw + tw - 1u) / tw;
-        atomicAdd(&a.st->unit_tiles, unit_tiles);
+        atomicAdd(&a.st->hot_tiles, hot_tiles);
         atomicAdd(&a.st->all_tiles, mine * (a.block_frames / MIX_TILE));
     }
 }

@@ -363,7 +363,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     ra.env_floor = c.env_floor;
     ra.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
     ra.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
-    const bool dbl = c.unit_tile_frames == 32 || (c.unit_tile_frames == 0 && s->unit_tiles);
+    const bool dbl = c.unit_tile_frames == 32 || (c.unit_tile_frames == 0 && s->hot_tiles);
     void* fn = render_table(c.interpolation, chan_active != 0, c.strict_fp != 0, c.mix_mode, s->vpl, dbl);
     void* args[] = {&ra};
     KC_CUDA(cudaLaunchKernel(fn, dim3(s->render_ctas), dim3(RENDER_WARPS * 32), args, s->render_smem, q));
@@ -661,7 +661,7 @@ int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out) {
     if (e != cudaSuccess) return bail(e);
     s->parity = 0;
     s->stats = src->stats;
-    s->unit_tiles = src->unit_tiles;
+    s->hot_tiles = src->hot_tiles;
     *out = s;
     return KC_OK;
 }
@@ -794,7 +794,7 @@ int kc_render_end(kc_synth* s, float* out, size_t n) {
     s->pending = false;
     std::memcpy(out, s->h_out, samples * 4);
     s->stats.active_voices = s->h_st->live;
-    if (s->h_st->all_tiles) s->unit_tiles = (uint64_t)s->h_st->unit_tiles * 2u >= s->h_st->all_tiles;
+    if (s->h_st->all_tiles) s->hot_tiles = (uint64_t)s->h_st->hot_tiles * 2u >= s->h_st->all_tiles;
     s->stats.stolen = s->h_st->stolen;
     s->stats.dropped = s->h_st->dropped;
     uint32_t pb = s->h_st->peak_bits;
@@ -869,7 +869,7 @@ int kc_synchronize(kc_synth* s) {
     KC_CUDA(cudaStreamSynchronize(s->stream));
     drain_timings(s);
     s->stats.active_voices = s->h_st->live;
-    if (s->h_st->all_tiles) s->unit_tiles = (uint64_t)s->h_st->unit_tiles * 2u >= s->h_st->all_tiles;
+    if (s->h_st->all_tiles) s->hot_tiles = (uint64_t)s->h_st->hot_tiles * 2u >= s->h_st->all_tiles;
     s->stats.stolen = s->h_st->stolen;
     s->stats.dropped = s->h_st->dropped;
     uint32_t pb = s->h_st->peak_bits;
@@ -902,9 +902,9 @@ int kc_last_block_voices(kc_synth* s, uint32_t* rendered) {
     return KC_OK;
 }
 
-int kc_last_block_tiles(kc_synth* s, uint32_t* unit_tiles, uint32_t* all_tiles) {
-    if (!s || !unit_tiles || !all_tiles) return fail(KC_ERR_INVALID, "null argument");
-    *unit_tiles = s->h_st->unit_tiles;
+int kc_last_block_tiles(kc_synth* s, uint32_t* hot_tiles, uint32_t* all_tiles) {
+    if (!s || !hot_tiles || !all_tiles) return fail(KC_ERR_INVALID, "null argument");
+    *hot_tiles = s->h_st->hot_tiles;
     *all_tiles = s->h_st->all_tiles;
     return KC_OK;
 }

@@ -75,9 +75,9 @@ struct kc_synth {
     // device; the staging writers wait on it before overwriting them.
     bool pending = false;
     cudaEvent_t ev_inputs = nullptr;
-    // Render with 32-frame unit tiles: set when most of the last block read
-    // back ran on the unit or integral-step path.
-    bool unit_tiles = false;
+    // Render with 32-frame hot tiles: set when most of the last block read
+    // back ran on a hot path (unit, integral or fractional step).
+    bool hot_tiles = false;
 
     // host mirror of BlockStats
     kc_block_stats stats{};

@@ -119,9 +119,10 @@ def test_sort_radix_widths_agree():
 @gpu
 @pytest.mark.parametrize("steps,chan", [("unit", True), ("integral", False), (None, True)])
 def test_unit_tile_lengths_agree(steps, chan):
-    """16-frame and 32-frame unit tiles, and the per-block choice between
-    them, leave byte-identical blocks and pools; the 32-frame form against
-    the CPU reference as well."""
+    """16-frame and 32-frame hot tiles (unit, integral and, with the default
+    steps, fractional), and the per-block choice between them, leave
+    byte-identical blocks and pools; the 32-frame form against the CPU
+    reference as well."""
     from kestrel_b200.backend import CudaSynth
     ref = None
     for utf in (16, 32, 0):
