@@ -151,14 +151,21 @@ def measured_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def render_profile_per_unit(key: str = "dram_bytes_per_voice_sample") -> float | None:
+# The render path a workload's blocks run on (at the f32 tree mix), and so
+# the captured case whose per-voice-sample figures describe its launch.
+PROFILE_PATH = {"steal": "unit", "steal-bent": "fractional"}
+
+
+def render_profile_per_unit(workload: str, mix_mode: int, key: str = "dram_bytes_per_voice_sample") -> float | None:
     """A per-voice-sample figure of the render kernel from the committed ncu
-    summary of it at this workload (profiles/render_traffic.json): DRAM bytes
-    read + written, or lane instructions issued."""
+    summary of the render path this workload runs on
+    (profiles/render_traffic.json): DRAM bytes read + written, or lane
+    instructions issued. None for workloads with no captured path."""
+    path = PROFILE_PATH.get(workload) if mix_mode == 0 else None
     p = ROOT / "profiles" / "render_traffic.json"
-    if p.exists():
+    if path and p.exists():
         try:
-            return float(json.loads(p.read_text())[key])
+            return float(json.loads(p.read_text())["paths"][path][key])
         except Exception:
             return None
     return None
@@ -614,8 +621,8 @@ def main(argv=None):
         n_render_mean = r["mean_live"]
         bytes_launch = render_algorithmic_bytes(int(round(n_render_mean)), r["bf"], r["tiles"])
         achieved = bytes_launch / (r["render_ms"] * 1e-3) / 1e9 if r["render_ms"] > 0 else 0.0
-        tpu = render_profile_per_unit()
-        ipu = render_profile_per_unit("lane_instructions_per_voice_sample")
+        tpu = render_profile_per_unit(args.workload, args.mix_mode)
+        ipu = render_profile_per_unit(args.workload, args.mix_mode, "lane_instructions_per_voice_sample")
         sms = torch_sm_count()
         value = units / (ms_t * 1e-3)
         line = {
