@@ -22,7 +22,14 @@ answers that need neither, each derived from a statement of the reference:
 * the biquad's impulse response is the f64 recursion's within a stated bound
   (src/cpu.rs:564-572);
 * a non-looping voice dies on the frame its phase reaches the sample's end
-  (src/cpu.rs:499-506).
+  (src/cpu.rs:499-506);
+* nearest interpolation reads the tap under the phase, and Catmull-Rom
+  follows its polynomial over the four taps advance_index picks, across the
+  loop seam (src/cpu.rs:240-302);
+* the steal set is the `need` smallest keys -- note ids under Oldest,
+  (level quantised to 16 bits, id) under Quietest -- each victim stopping at
+  id % span + 1 and fading out, and compaction keeps the survivors' order
+  (src/cpu.rs:213-221, 330-391, 84-117).
 
 Every case runs on the oracle (CPU suite) and on the CUDA backend (marked
 gpu). One voice sounds at a time, with gain 1.0 unless stated, so the output
@@ -433,3 +440,113 @@ def test_end_of_sample_kill_frame(kind):
     x = tap(16384)
     assert np.all(left[:800] == x) and np.all(left[800:] == 0.0)
     assert fields.shape[1] == 0
+
+
+# ---- src/cpu.rs:240-302: nearest and Catmull-Rom, loop-aware neighbours ---------------------------
+
+def _ramp_voice(cfg_interp, kind, blocks=2):
+    L, ls, le = 3000, 1000, 3000
+    ramp = (-30000 + 20 * np.arange(L)).astype(np.int16)  # exactly linear in i16
+    pool = np.concatenate([ramp, np.zeros(8, np.int16)])
+    step, start = 0x1_3C6E_F372, (5 << 32) | 0x2468_ACE0
+    cfg = N.default_config(max_voices=8, interpolation=cfg_interp)
+    left, _, fields = render(kind, cfg, pool, instant_params(), one_voice(L, step, start, loop=(ls, le)), blocks)
+    frames = blocks * cfg.block_frames
+    ph = [closed_phase(start, step, f, ls, le) for f in range(frames)]
+    idx = np.array([p[0] for p in ph], np.int64)
+    fr = np.array([p[1] for p in ph], np.uint64).astype(F32) * F32(1.0 / 4294967296.0)
+    return left, fields, ramp, idx, fr, (ls, le), (start, step, frames)
+
+
+@pytest.mark.parametrize("kind", BACKENDS)
+def test_nearest_reads_the_tap_under_the_phase(kind):
+    left, fields, ramp, idx, _, (ls, le), (start, step, frames) = _ramp_voice(N.INTERP_NEAREST, kind)
+    np.testing.assert_array_equal(left, tap(ramp[idx]))
+    assert (int(fields[N.FIELD["phase_hi"], 0]), int(fields[N.FIELD["phase_lo"], 0])) == \
+        closed_phase(start, step, frames, ls, le)
+
+
+@pytest.mark.parametrize("kind", BACKENDS)
+def test_catmull_rom_follows_its_polynomial_across_the_loop_seam(kind):
+    # Every frame against catmull_rom (src/cpu.rs:295-302) of the four taps
+    # advance_index picks (src/cpu.rs:240-259: index - 1, + 1, + 2, wrapped
+    # into [loop_start, loop_end)), evaluated in f64: within 4e-6 (a few f32
+    # roundings of values up to 2). On the exactly linear stretch of the ramp
+    # the polynomial is the straight line; across the seam it blends the
+    # loop's end into its start.
+    left, _, ramp, idx, fr, (ls, le), _ = _ramp_voice(N.INTERP_CUBIC, kind)
+
+    def nb(i, off):
+        raw = i + off
+        return np.where(raw >= le, ls + (raw - ls) % (le - ls), np.maximum(raw, 0))
+
+    t = [tap(ramp[nb(idx, o)]).astype(np.float64) for o in (-1, 0, 1, 2)]
+    f = fr.astype(np.float64)
+    a = -0.5 * t[0] + 1.5 * t[1] - 1.5 * t[2] + 0.5 * t[3]
+    b = t[0] - 2.5 * t[1] + 2.0 * t[2] - 0.5 * t[3]
+    c = -0.5 * t[0] + 0.5 * t[2]
+    want = ((a * f + b) * f + c) * f + t[1]
+    assert np.max(np.abs(left - want)) <= 4e-6
+    seam = (idx >= le - 2) | (idx < ls + 1)
+    assert seam.sum() > 10  # the seam was crossed
+    lin = ~seam
+    line = t[1] + (t[2] - t[1]) * f
+    assert np.max(np.abs(left[lin] - line[lin])) <= 4e-6
+
+
+# ---- src/cpu.rs:330-391: the steal set ------------------------------------------------------------
+
+def _steal_run(kind, rule, params, which_params):
+    """64 sustained voices (note ids 1..64) fill a 64-voice pool in block 0;
+    block 1 spawns 10 more (ids 65..74), so 10 must be stolen (max_steal 16).
+    Every voice is full scale at gain 2^-7, so the block's sums are exact."""
+    cfg = N.default_config(max_voices=64, max_steal_percent=25, steal_rule=rule, sort_voices=0)
+    ids = np.arange(1, 75)
+    cmds = np.concatenate([one_voice(56, loop=(0, 56), note_id_lo=i, gain_l=2.0**-7, gain_r=2.0**-7,
+                                     params=which_params(i)) for i in ids])
+    s = make_backend(kind, cfg, DC_POOL, params)
+    tiles = cfg.block_frames // cfg.gate_frames
+    outs, live_ids = [], []
+    try:
+        for b, batch in enumerate((cmds[:64], cmds[64:])):
+            s.set_gates(np.zeros(tiles * N.GATE_SLOTS, np.uint32))
+            s.set_channels(np.zeros(tiles * 64, np.uint32), False, False, False)
+            s.spawn(batch)
+            outs.append(s.render().copy().reshape(-1, 2)[:, 0])
+            live_ids.append(s.read_pool()[N.FIELD["note_lo"]].astype(np.int64))
+        st = s.stats()
+    finally:
+        s.close()
+    return outs, live_ids, st, cfg
+
+
+@pytest.mark.parametrize("kind", BACKENDS)
+def test_oldest_rule_steals_the_lowest_note_ids(kind):
+    outs, live, st, cfg = _steal_run(kind, N.STEAL_OLDEST, instant_params(), lambda i: 0)
+    assert (st.stolen, st.dropped, st.active_voices) == (10, 0, 64)
+    # Victims are ids 1..10: each stops at frame id % span + 1 and fades over
+    # steal_fade_frames, then is compacted away; the survivors keep their order.
+    np.testing.assert_array_equal(live[1], np.arange(11, 75))
+    span = cfg.block_frames - cfg.steal_fade_frames
+    assert all(i % span + 1 == i + 1 for i in range(1, 11))
+    assert outs[1][0] == F32(74 * 2.0**-7)           # every voice at full level on frame 0
+    assert np.all(outs[1][10 + 96:] == F32(64 * 2.0**-7))  # the last victim (id 10) is silent from frame 106
+    # id 1 stops at frame 2 (stop_rel 2): d = f + 1 - 2 is 0 on frame 1 and 1 on frame 2
+    assert outs[1][1] == outs[1][0] and outs[1][2] < outs[1][1]
+
+
+@pytest.mark.parametrize("kind", BACKENDS)
+def test_quietest_rule_steals_the_lowest_levels_then_ids(kind):
+    # Four sustain levels; a voice's steal key is its level quantised to 16
+    # bits above its note id (src/cpu.rs:213-221), so the victims are the 10
+    # smallest (level, id) pairs.
+    sus = np.array([0.75, 0.25, 1.0, 0.5], np.float32)
+    params = np.concatenate([instant_params(decay_target=s, sustain=s) for s in sus])
+    pick = lambda i: (i * 7) % 4
+    outs, live, st, _ = _steal_run(kind, N.STEAL_QUIETEST, params, pick)
+    assert (st.stolen, st.dropped, st.active_voices) == (10, 0, 64)
+    q = {i: int(np.float32(sus[pick(i)]) * np.float32(65535.0)) for i in range(1, 65)}
+    victims = sorted(range(1, 65), key=lambda i: (q[i], i))[:10]
+    assert all(sus[pick(i)] == np.float32(0.25) for i in victims)
+    want = [i for i in range(1, 65) if i not in victims] + list(range(65, 75))
+    np.testing.assert_array_equal(live[1], want)
