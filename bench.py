@@ -71,6 +71,8 @@ def parse_args(argv=None):
     ap.add_argument("--voices-per-lane", type=int, default=0)
     ap.add_argument("--strict-fp", type=int, default=1)
     ap.add_argument("--mix-mode", type=int, default=0, help="0 f32 tree, 1 compensated two-sum, 2 FP64")
+    ap.add_argument("--tile-frames", type=int, default=0,
+                    help="longest render tile on the hot paths: 16, 32 or 0 = chosen per block")
     return ap.parse_args(argv)
 
 
@@ -202,6 +204,7 @@ def run_cuda(args, world, rank, local):
     cfg.voices_per_lane = args.voices_per_lane
     cfg.strict_fp = args.strict_fp
     cfg.mix_mode = args.mix_mode
+    cfg.unit_tile_frames = args.tile_frames
     bank = H.Bank(bs, cfg)
     drv = H.Driver(cfg, bank, ms)
     A = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)

@@ -895,7 +895,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 }
                 if (!carry_left) path = classify<INTERP, V, 16>(v, a, f0, looping, active, e, fm);
                 carried = path;
-                if (path <= P_HOT) hot_tiles += carry_left + 1u;
+
             }
             // A hot tile (unit, integral or fractional step) whose successor
             // is in the same span and behind no gate row runs with it as one
@@ -907,6 +907,9 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                 --carry_left;
                 if (!first) part_prev2 = part[j + 2u * MIX_TILE];
             }
+            // counted as run (a carried span cut short by a gate row is
+            // classified again, so counting it ahead would count tiles twice)
+            if (path <= P_HOT) hot_tiles += nt / MIX_TILE;
             if (path <= P_HOT) {
                 bool done = false;
                 if constexpr (DOUBLE) {

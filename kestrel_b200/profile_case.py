@@ -31,10 +31,12 @@ def main(argv=None) -> int:
     ap.add_argument("--unity", type=int, default=0, help="1: every voice at exactly unity step")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--vpl", type=int, default=0, help="voices per lane (0 = default)")
+    ap.add_argument("--tile", type=int, default=0, help="longest hot tile in frames: 16, 32 or 0 = per block")
     args = ap.parse_args(argv)
 
     nv = args.voices
-    cfg = N.default_config(max_voices=nv, sort_voices=args.sort, strict_fp=args.strict, voices_per_lane=args.vpl)
+    cfg = N.default_config(max_voices=nv, sort_voices=args.sort, strict_fp=args.strict, voices_per_lane=args.vpl,
+                           unit_tile_frames=args.tile)
     bank = H.Bank(H.bank_spec(presets=1), cfg)
     rng = np.random.default_rng(args.seed)
     params = bank.params.copy()
@@ -80,7 +82,7 @@ def main(argv=None) -> int:
         t = dict(s.timings())
         live = s.stats().active_voices
         rate = live * cfg.block_frames / (t["render"] * 1e-3) if t.get("render") else 0.0
-        print(f"vpl={args.vpl} strict={args.strict} chan={args.chan} unity={args.unity} block {b}: live {live} render {t.get('render', 0):.3f} ms "
+        print(f"vpl={args.vpl} tile={args.tile} strict={args.strict} chan={args.chan} unity={args.unity} block {b}: live {live} render {t.get('render', 0):.3f} ms "
               f"({rate:.3e} voice-frames/s) " + " ".join(f"{k}={v:.3f}" for k, v in t.items()), flush=True)
     s.close()
     return 0
