@@ -71,6 +71,8 @@ def parse_args(argv=None):
     ap.add_argument("--voices-per-lane", type=int, default=0)
     ap.add_argument("--strict-fp", type=int, default=1)
     ap.add_argument("--mix-mode", type=int, default=0, help="0 f32 tree, 1 compensated two-sum, 2 FP64")
+    ap.add_argument("--sort-every", type=int, default=1,
+                    help="re-sort the voice pool every N blocks (compact it on the others); 0 never")
     ap.add_argument("--tile-frames", type=int, default=0,
                     help="longest render tile on the hot paths: 16, 32 or 0 = chosen per block")
     return ap.parse_args(argv)
@@ -205,6 +207,7 @@ def run_cuda(args, world, rank, local):
     cfg.strict_fp = args.strict_fp
     cfg.mix_mode = args.mix_mode
     cfg.unit_tile_frames = args.tile_frames
+    cfg.sort_voices = args.sort_every
     bank = H.Bank(bs, cfg)
     drv = H.Driver(cfg, bank, ms)
     A = CudaSynth(cfg, bank.pool, bank.params, bank.regions, bank.max_sample_len)
@@ -266,6 +269,7 @@ def run_cuda(args, world, rank, local):
         enqueue(e)
     B.synchronize()
     B.set_profile(True)
+    launches0 = B.launches_total()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -286,7 +290,7 @@ def run_cuda(args, world, rank, local):
     units = sum(n for _, n, *_ in dev[W:]) * bf
     # determinism: the replay must equal the host-buffer render byte for byte
     same = all(np.array_equal(e[5].cpu().numpy(), outs_a[i]) for i, e in enumerate(dev))
-    launches = B.block_launches() * K
+    launches = B.launches_total() - launches0  # kernel launches of the K timed blocks
 
     res = {
         "units": units, "ms": dt_ms, "e2e_units": e2e_units, "e2e_s": e2e_t, "h2d": h2d // max(K, 1),
@@ -499,7 +503,7 @@ def bench_config(args, world):
     cfg, _, _ = H.config_workload(args.workload, seed=args.seed)
     return {"workload": workload_desc(args.workload), "block_frames": cfg.block_frames,
             "sample_rate": cfg.sample_rate, "max_voices": cfg.max_voices,
-            "mix": ["f32 tree", "two-sum", "f64"][args.mix_mode],
+            "mix": ["f32 tree", "two-sum", "f64"][args.mix_mode], "pool_sort_every": args.sort_every,
             "parallelism": "replicas" if world > 1 else "single",
             "l2": "inputs larger than L2 (voice pool >= 1.8 GB at 8.4M voices)"
                   if args.workload.startswith("steal") else "inputs smaller than L2 between blocks"}

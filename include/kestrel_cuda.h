@@ -136,7 +136,9 @@ typedef struct kc_config {
     uint32_t decay_curve;        /* KC_CURVE_*, Exponential */
     uint32_t release_curve;      /* KC_CURVE_*, Exponential */
     float env_floor;             /* 1e-5 */
-    uint32_t sort_voices;        /* 1: re-sort the pool by (region, stage, phase) */
+    uint32_t sort_voices;        /* N > 0: re-sort the pool by (region, stage, phase) on every
+                                    Nth block (1: every block, the default), compact it in
+                                    place of the sort on the others; 0: never sort */
     uint32_t max_param_variants; /* params-table copies, 32 */
     uint32_t mix_mode;           /* KC_MIX_*, F32 tree */
     uint32_t strict_fp;          /* 1: no FMA contraction anywhere in the voice DSP */
@@ -196,7 +198,9 @@ int kc_set_params_variant(kc_synth* s, uint32_t index, const kc_region_params* d
                           size_t n);
 
 /* Backend::spawn (src/backend.rs:41-43). The commands are validated and
- * copied; steal/drop/admit happen on the device inside the next render. */
+ * copied; steal/drop/admit happen on the device inside the next render. A
+ * refused call (a params index or gate slot out of range) leaves no commands
+ * staged. */
 int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n);
 
 /* Backend::render (src/backend.rs:45-47): `out` receives block_frames * 2
@@ -245,8 +249,11 @@ int kc_enqueue_block_device(kc_synth* s, const uint32_t* d_gates, const uint32_t
 int kc_synchronize(kc_synth* s);
 /* The context's cudaStream_t, for event timing by the caller. */
 void* kc_stream(kc_synth* s);
-/* Number of kernel launches one block enqueues (the captured graph's nodes). */
+/* Number of kernel launches one block enqueues when it sorts the pool (the
+ * captured graph's nodes), and the launches this context's blocks have
+ * enqueued so far. */
 int kc_block_launches(kc_synth* s, uint32_t* out);
+int kc_launches_total(kc_synth* s, uint64_t* out);
 
 /* ---- precision form ------------------------------------------------------ *
  * RBJ lowpass coefficients designed in FP64 on the device: `coefs` receives

@@ -195,6 +195,12 @@ class CudaSynth:
         N.check(self._lib.kc_last_block_voices(self._h, C.byref(n)), self._lib)
         return n.value
 
+    def launches_total(self) -> int:
+        """Kernel launches this context's blocks have enqueued so far."""
+        n = C.c_uint64()
+        N.check(self._lib.kc_launches_total(self._h, C.byref(n)), self._lib)
+        return n.value
+
     def last_block_tiles(self) -> tuple[int, int]:
         """(hot-path warp-tiles -- unit, integral or fractional step -- and all
         warp-tiles) of the last block."""

@@ -717,7 +717,8 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         d.want = s->want;
         d.chan_active = (s->bend ? 1u : 0u) | (s->gain ? 2u : 0u) | (s->variant ? 4u : 0u);
         d.samples = c.block_frames * 2;
-        d.sort_passes = c.sort_voices ? (s->sort.bits + s->radix - 1) / s->radix : 0u;
+        d.sort_passes = sort_this_block(s) ? (s->sort.bits + s->radix - 1) / s->radix : 0u;
+        ++s->blocks;
         d.sel_cap = s->pool_ctas;
         d.cmp_cap = s->compact_ctas;
     }

@@ -279,15 +279,21 @@ __device__ __forceinline__ void scan_counts_body(uint32_t* counts, uint32_t m, u
     if (threadIdx.x == 0) *total = carry;
 }
 
-__device__ __forceinline__ void copy_voice(const uint32_t* src, uint32_t* dst, uint32_t cap, uint32_t from,
-                                           uint32_t to) {
+// The two pool buffers never overlap, so every field is loaded before any is
+// stored: 21 loads in flight per thread instead of a load-store chain the
+// compiler would have to keep in order for possibly aliasing pointers.
+__device__ __forceinline__ void copy_voice(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t cap,
+                                           uint32_t from, uint32_t to) {
+    uint32_t w[VOICE_FIELDS];
 #pragma unroll
-    for (uint32_t f = 0; f < VOICE_FIELDS; ++f) dst[f * cap + to] = src[f * cap + from];
-    // Start offset, born-under variant and stop frame apply only to the block
-    // a voice was born or stolen in (shaders/compact.wgsl:134-138).
-    dst[F_START_REL * cap + to] = 0u;
-    dst[F_BORN_VARIANT * cap + to] = 0u;
-    dst[F_STOP_REL * cap + to] = 0u;
+    for (uint32_t f = 0; f < VOICE_FIELDS; ++f) {
+        // Start offset, born-under variant and stop frame apply only to the
+        // block a voice was born or stolen in (shaders/compact.wgsl:134-138).
+        const bool cleared = f == F_START_REL || f == F_BORN_VARIANT || f == F_STOP_REL;
+        w[f] = cleared ? 0u : __ldg(src + (size_t)f * cap + from);
+    }
+#pragma unroll
+    for (uint32_t f = 0; f < VOICE_FIELDS; ++f) dst[(size_t)f * cap + to] = w[f];
 }
 
 __device__ __forceinline__ void compact_scatter_body(PoolArgs a, const uint32_t* offsets, uint32_t cta,

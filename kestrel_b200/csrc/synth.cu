@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -267,6 +268,7 @@ void free_all(kc_synth* s) {
     for (auto& set : s->ring)
         for (auto& e : set) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
 }
 
 // Config::validate (src/config.rs:412-525), the part the backend reads, plus
@@ -296,8 +298,13 @@ int validate(const kc_config& c) {
 }
 
 // Enqueue one block on the stream. All inputs are device pointers.
+uint32_t launches_for(const kc_synth* s, bool sort_now);
+
+// `inputs_ready` (optional): an event the spawn pass waits for, recorded
+// after the block's inputs were copied up on another stream.
 int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, bool bend, bool gain,
-                  bool variant, const kc_spawn_cmd* d_cmds, uint32_t n_cmds, float* d_out) {
+                  bool variant, const kc_spawn_cmd* d_cmds, uint32_t n_cmds, float* d_out,
+                  cudaEvent_t inputs_ready = nullptr) {
     cudaStream_t q = s->stream;
     const kc_config& c = s->cfg;
     const uint32_t chan_active = (bend ? 1u : 0u) | (gain ? 2u : 0u) | (variant ? 4u : 0u);
@@ -338,6 +345,7 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     }
     if (s->profile) cudaEventRecord(ev[1], q);
     // ---- 2. spawn ----
+    if (inputs_ready) KC_CUDA(cudaStreamWaitEvent(q, inputs_ready, 0));
     k_spawn<<<s->pool_ctas, 256, 0, q>>>(pa, d_cmds);
     if (s->profile) cudaEventRecord(ev[2], q);
     // ---- 3. render ----
@@ -381,7 +389,8 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     k_compact_count<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
     k_scan_counts<<<1, 1024, 0, q>>>(s->counts, s->compact_ctas, s->total);
     k_commit<<<1, 1, 0, q>>>(s->st, s->total);
-    if (!c.sort_voices) {
+    const bool sort_now = sort_this_block(s);
+    if (!sort_now) {
         k_compact_scatter<<<s->compact_ctas, 256, 0, q>>>(pa, s->counts);
     } else {
         const uint32_t passes = (s->sort.bits + s->radix - 1) / s->radix;
@@ -400,6 +409,8 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     if (s->profile) cudaEventRecord(ev[5], q);
     KC_CUDA(cudaGetLastError());
     s->parity ^= 1;
+    s->launches += launches_for(s, sort_now);
+    ++s->blocks;
     return KC_OK;
 }
 
@@ -419,12 +430,15 @@ void drain_timings(kc_synth* s) {
     s->ring_pending = 0;
 }
 
-uint32_t launches_per_block(const kc_synth* s) {
+}  // namespace
+
+namespace {
+uint32_t launches_for(const kc_synth* s, bool sort_now) {
     uint32_t n = 1;                                                       // admit
     if (s->cfg.steal_rule != KC_STEAL_DROP_NEW) n += 2 * SEL_ROUNDS + 1;  // select + mark
     n += 1 + 1 + 1;                                                       // spawn, render, reduce
     n += 3;                                                               // count, scan, commit
-    if (!s->cfg.sort_voices) n += 1;
+    if (!sort_now) n += 1;
     else n += 3 * ((s->sort.bits + s->radix - 1) / s->radix) + 1;
     return n;
 }
@@ -530,6 +544,7 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     KC_TRY(cudaSetDevice(s->device));
     KC_TRY(cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, s->device));
     KC_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    KC_TRY(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
 
     s->cap = (uint32_t)((slots + 31) & ~31ull);
     s->vpl = cfg->voices_per_lane == 2 ? 2u : 1u;
@@ -661,6 +676,7 @@ int kc_synth_clone_config(kc_synth* src, const kc_config* cfg, kc_synth** out) {
     if (e != cudaSuccess) return bail(e);
     s->parity = 0;
     s->stats = src->stats;
+    s->blocks = src->blocks;  // the pool-sort interval continues where the source's stands
     s->hot_tiles = src->hot_tiles;
     *out = s;
     return KC_OK;
@@ -724,12 +740,6 @@ int kc_set_params_variant(kc_synth* s, uint32_t index, const kc_region_params* d
 int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n) {
     if (!s || (!cmds && n)) return fail(KC_ERR_INVALID, "null argument");
     if (n > 0x7FFFFFFFull) return fail(KC_ERR_INVALID, "too many spawn commands");
-    // The CPU backend indexes these tables directly and would panic on a bad
-    // index; reject them here instead of reading out of bounds on the device.
-    for (size_t i = 0; i < n; ++i) {
-        if (cmds[i].params >= s->params_per) return fail(KC_ERR_INVALID, "spawn command params index out of range");
-        if (cmds[i].gate_slot >= KC_GATE_SLOTS) return fail(KC_ERR_INVALID, "spawn command gate_slot out of range");
-    }
     if (int rc = staging_free(s)) return rc;
     if (n > s->h_cmds_cap) {
         cudaSetDevice(s->device);
@@ -743,7 +753,37 @@ int kc_spawn(kc_synth* s, const kc_spawn_cmd* cmds, size_t n) {
             return fail(KC_ERR_OOM, "pinned spawn staging");
         s->h_cmds_cap = nc;
     }
-    if (n) std::memcpy(s->h_cmds, cmds, n * sizeof(kc_spawn_cmd));
+    // The CPU backend indexes the params and gate tables directly and would
+    // panic on a bad index; reject such commands here instead of reading out
+    // of bounds on the device. Validation and the copy into pinned staging run
+    // together, split over a few threads for large blocks (a saturated
+    // block's commands are megabytes); a refused call leaves no commands
+    // staged.
+    s->want = 0;
+    const size_t chunk = (size_t)1 << 15;
+    const unsigned workers = n >= 2 * chunk ? (unsigned)std::min<size_t>(4, n / chunk) : 1u;
+    std::vector<int> bad(workers, 0);
+    auto part = [&](unsigned w) {
+        const size_t lo = n * w / workers, hi = n * (w + 1) / workers;
+        for (size_t i = lo; i < hi; ++i)
+            if (cmds[i].params >= s->params_per || cmds[i].gate_slot >= KC_GATE_SLOTS) {
+                bad[w] = cmds[i].params >= s->params_per ? 1 : 2;
+                return;
+            }
+        std::memcpy(s->h_cmds + lo, cmds + lo, (hi - lo) * sizeof(kc_spawn_cmd));
+    };
+    if (workers == 1) {
+        if (n) part(0);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned w = 1; w < workers; ++w) th.emplace_back(part, w);
+        part(0);
+        for (auto& t : th) t.join();
+    }
+    for (int b : bad) {
+        if (b == 1) return fail(KC_ERR_INVALID, "spawn command params index out of range");
+        if (b == 2) return fail(KC_ERR_INVALID, "spawn command gate_slot out of range");
+    }
     s->want = (uint32_t)n;
     return KC_OK;
 }
@@ -769,13 +809,19 @@ int kc_render_begin(kc_synth* s) {
     const size_t samples = (size_t)s->cfg.block_frames * 2;
     const size_t gate_words = (size_t)s->tiles * KC_GATE_SLOTS;
     const size_t chan_words = (size_t)s->tiles * KC_BEND_CHANNELS * KC_CHAN_FIELDS;
-    KC_CUDA(cudaMemcpyAsync(s->gates, s->h_gates, gate_words * 4, cudaMemcpyHostToDevice, q));
-    KC_CUDA(cudaMemcpyAsync(s->chan, s->h_chan, chan_words * 4, cudaMemcpyHostToDevice, q));
+    // The inputs go up on the copy stream while the block's admission and
+    // steal select (which read none of them) run; the spawn pass waits for
+    // them. Nothing of an earlier block reads these buffers any more: a block
+    // begun here has been ended (synchronised) before the next begins.
+    cudaStream_t cq = s->copy_stream;
+    KC_CUDA(cudaMemcpyAsync(s->gates, s->h_gates, gate_words * 4, cudaMemcpyHostToDevice, cq));
+    KC_CUDA(cudaMemcpyAsync(s->chan, s->h_chan, chan_words * 4, cudaMemcpyHostToDevice, cq));
     if (s->want)
         KC_CUDA(cudaMemcpyAsync(s->cmds, s->h_cmds, (size_t)s->want * sizeof(kc_spawn_cmd),
-                                cudaMemcpyHostToDevice, q));
-    KC_CUDA(cudaEventRecord(s->ev_inputs, q));
-    if (int rc = enqueue_block(s, s->gates, s->chan, s->bend, s->gain, s->variant, s->cmds, s->want, s->out))
+                                cudaMemcpyHostToDevice, cq));
+    KC_CUDA(cudaEventRecord(s->ev_inputs, cq));
+    if (int rc = enqueue_block(s, s->gates, s->chan, s->bend, s->gain, s->variant, s->cmds, s->want, s->out,
+                               s->ev_inputs))
         return rc;
     KC_CUDA(cudaMemcpyAsync(s->h_out, s->out, samples * 4, cudaMemcpyDeviceToHost, q));
     KC_CUDA(cudaMemcpyAsync(s->h_st, s->st, sizeof(DevState), cudaMemcpyDeviceToHost, q));
@@ -882,7 +928,7 @@ void* kc_stream(kc_synth* s) { return s ? (void*)s->stream : nullptr; }
 
 int kc_block_launches(kc_synth* s, uint32_t* out) {
     if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
-    *out = launches_per_block(s);
+    *out = launches_for(s, true);
     return KC_OK;
 }
 
@@ -899,6 +945,12 @@ int kc_device_memory(int device, uint64_t* free_bytes, uint64_t* total_bytes) {
 int kc_last_block_voices(kc_synth* s, uint32_t* rendered) {
     if (!s || !rendered) return fail(KC_ERR_INVALID, "null argument");
     *rendered = s->h_st->live_render;
+    return KC_OK;
+}
+
+int kc_launches_total(kc_synth* s, uint64_t* out) {
+    if (!s || !out) return fail(KC_ERR_INVALID, "null argument");
+    *out = s->launches;
     return KC_OK;
 }
 

@@ -14,11 +14,20 @@ namespace kc {
 constexpr int N_TIMERS = 5;
 }  // namespace kc
 
+struct kc_synth;
+namespace kc {
+// Does the next block re-sort the pool (Config::sort_voices every Nth block:
+// 1 = every block, 0 = never) or only compact it? Both leave the same voices;
+// the sort only orders them for the render's locality.
+bool sort_this_block(const kc_synth* s);
+}  // namespace kc
+
 struct kc_synth {
     kc_config cfg{};
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // the host-buffer inputs' uploads (kc_render_begin)
 
     uint32_t cap = 0;           // pool slots, padded to 32
     uint32_t tiles = 0;         // gate tiles per block
@@ -79,6 +88,11 @@ struct kc_synth {
     // back ran on a hot path (unit, integral or fractional step).
     bool hot_tiles = false;
 
+    // Blocks enqueued on this context (its own render or a batch's), which
+    // times the pool sort's interval, and kernel launches its renders enqueued.
+    uint64_t blocks = 0;
+    uint64_t launches = 0;
+
     // host mirror of BlockStats
     kc_block_stats stats{};
 
@@ -93,3 +107,9 @@ struct kc_synth {
     double total_ms[kc::N_TIMERS] = {};
     uint64_t total_blocks = 0;
 };
+
+namespace kc {
+inline bool sort_this_block(const kc_synth* s) {
+    return s->cfg.sort_voices != 0 && s->blocks % s->cfg.sort_voices == 0;
+}
+}  // namespace kc

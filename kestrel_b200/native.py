@@ -161,6 +161,7 @@ CUDA_SYMBOLS = {
     "kc_estimate_device_bytes": (C.c_int, [C.POINTER(KcConfig), C.c_uint64, C.c_uint32, C.POINTER(C.c_uint64)]),
     "kc_last_block_voices": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "kc_last_block_tiles": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "kc_launches_total": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "kc_device_memory": (C.c_int, [C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "kc_render_block_noalloc": (C.c_int, [C.POINTER(KcConfig), _P, C.c_uint32, C.c_uint32, _P, C.c_uint64, _P,
                                           C.c_uint32, C.c_uint32, _P, _P, C.c_int, C.c_int, C.c_int, _P, _P]),

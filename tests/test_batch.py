@@ -24,11 +24,12 @@ def _jobs(strict_fp=1, mix_mode=N.MIX_F32_TREE, vpl=0):
         make_scenario(seed=21, max_voices=4096, n_blocks=6, **kw),
         make_scenario(seed=22, max_voices=512, n_blocks=5, spawn_per_block=(0, 400), steal_rule=N.STEAL_OLDEST,
                       admit_rule=N.ADMIT_EVEN, **kw),
+        # sorted every third block (compacted on the others)
         make_scenario(seed=23, max_voices=30000, n_blocks=4, spawn_per_block=(6000, 9000), release_rate=0.02,
-                      sort_voices=1, **kw),
+                      sort_voices=3, **kw),
         make_scenario(seed=24, max_voices=2048, n_blocks=6, chan=False, variants=0, steal_rule=N.STEAL_DROP_NEW,
                       **kw),
-        make_scenario(seed=25, max_voices=64, n_blocks=3, spawn_per_block=(0, 40), sort_voices=1, **kw),
+        make_scenario(seed=25, max_voices=64, n_blocks=3, spawn_per_block=(0, 40), sort_voices=2, **kw),
         make_scenario(seed=26, max_voices=8192, n_blocks=5, spawn_per_block=(0, 0), **kw),  # silent job
     ]
 
