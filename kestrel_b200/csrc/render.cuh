@@ -344,28 +344,69 @@ __device__ __forceinline__ bool fast_ok(const VoiceRegs& v, const RenderArgs& a,
     return true;
 }
 
+// Packed two-lane f32 arithmetic (sm_100 `.f32x2`): one instruction issues
+// both halves, and each half rounds exactly as the scalar `.rn` instruction
+// does. No packed add on this path consumes a packed product: the assembler
+// contracts such a pair into one packed FMA even with an explicit rounding
+// mode (measured: a strict biquad written that way left different filter
+// state), so every packed product here feeds scalar adds, another product or
+// an FMA's multiplicand.
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mul.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 fma2_rn(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pc, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mov.b64 pc, {%6, %7};\n\tfma.rn.f32x2 pd, pa, pb, pc;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+
 // The biquad (transposed direct form II, b2 == b0, src/cpu.rs:564-572) on one
-// sample.
-template <bool STRICT>
+// sample. PACKED issues each pair of independent products, (b0 x, b1 x) and
+// (a1 y, a2 y), as one packed multiply, with the same roundings: two
+// instructions fewer per frame. The unit- and integral-step hot tiles use it
+// (measured faster there); the fractional-step tile does not (every packed
+// form measured slower on that path).
+template <bool STRICT, bool PACKED = false>
 __device__ __forceinline__ float biquad_core(VoiceRegs& v, float x) {
     float y;
-    if (STRICT) {
+    if (STRICT && !PACKED) {
         const float bx = __fmul_rn(v.b0, x);
         y = __fadd_rn(bx, v.z1);
         v.z1 = __fadd_rn(__fsub_rn(__fmul_rn(v.b1, x), __fmul_rn(v.a1, y)), v.z2);
         v.z2 = __fsub_rn(bx, __fmul_rn(v.a2, y));
-    } else {
+    } else if (STRICT) {
+        const float2 bb = mul2_rn(make_float2(v.b0, v.b1), make_float2(x, x));
+        y = __fadd_rn(bb.x, v.z1);
+        const float2 ay = mul2_rn(make_float2(v.a1, v.a2), make_float2(y, y));
+        v.z1 = __fadd_rn(__fsub_rn(bb.y, ay.x), v.z2);
+        v.z2 = __fsub_rn(bb.x, ay.y);
+    } else if (!PACKED) {
         y = fmaf(v.b0, x, v.z1);
         v.z1 = fmaf(v.b1, x, fmaf(-v.a1, y, v.z2));
         v.z2 = fmaf(v.b0, x, -(v.a2 * y));
+    } else {
+        // (-a2 y) as fma(-a2, y, -0): the exact negated product.
+        y = __fmaf_rn(v.b0, x, v.z1);
+        const float2 z = fma2_rn(make_float2(v.b1, v.b0), make_float2(x, x),
+                                 fma2_rn(make_float2(-v.a1, -v.a2), make_float2(y, y), make_float2(v.z2, -0.0f)));
+        v.z1 = z.x;
+        v.z2 = z.y;
     }
     return y;
 }
 
 // y = x when the region's filter is off.
-template <bool STRICT>
+template <bool STRICT, bool PACKED = false>
 __device__ __forceinline__ float biquad(VoiceRegs& v, float x) {
-    return v.filt ? biquad_core<STRICT>(v, x) : x;
+    return v.filt ? biquad_core<STRICT, PACKED>(v, x) : x;
 }
 
 template <bool STRICT>
@@ -651,11 +692,11 @@ __device__ __forceinline__ void emit(float* sm, uint32_t lane, uint32_t i, const
     }
 }
 
-template <bool STRICT, int FM>
+template <bool STRICT, int FM, bool PACKED = false>
 __device__ __forceinline__ float biquad_fm(VoiceRegs& v, float x) {
     if (FM == FM_NONE) return x;
-    if (FM == FM_LANE) return biquad<STRICT>(v, x);
-    return biquad_core<STRICT>(v, x);  // FM_ALL: no per-lane test
+    if (FM == FM_LANE) return biquad<STRICT, PACKED>(v, x);
+    return biquad_core<STRICT, PACKED>(v, x);  // FM_ALL: no per-lane test
 }
 
 // Taps from a base index. The pointer is formed once, so a tap at a fixed
@@ -716,7 +757,7 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
-                y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(t[k][i], v[k].level));
+                y[k] = biquad_fm<STRICT, FM, true>(v[k], __fmul_rn(t[k][i], v[k].level));
             }
             emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
@@ -733,7 +774,7 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
-                y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(tap<F32>(a, off[k]), v[k].level));
+                y[k] = biquad_fm<STRICT, FM, true>(v[k], __fmul_rn(tap<F32>(a, off[k]), v[k].level));
                 off[k] += (uint32_t)(v[k].step >> 32);
             }
             emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
@@ -750,14 +791,20 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
         // subnormal -- so s0 + that is the reference's interpolation
         // (src/cpu.rs:279-283) bit for bit, in three operations instead of
         // five and one load instead of two.
-        uint64_t q[V];
+        // q is kept as two 32-bit words advanced by one add-with-carry pair,
+        // and the pair's address is one wide multiply-add of the high word:
+        // 3.7 instructions a frame fewer than the 64-bit add, shift and
+        // address arithmetic the compiler makes of q += step (measured).
+        uint32_t qh[V], ql[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) {
-            q[k] = v[k].phase + ((uint64_t)v[k].base << 32);
+            const uint64_t q = v[k].phase + ((uint64_t)v[k].base << 32);
+            qh[k] = (uint32_t)(q >> 32);
+            ql[k] = (uint32_t)q;
             // The next tile's first pair and the line after it: fast_ok
             // bounded the span's last index below pcm_len, and the table runs
             // ZERO_PAD entries past it.
-            const float2* nx = a.pcmp + (uint32_t)((q[k] + (v[k].step << LOG_NT)) >> 32);
+            const float2* nx = a.pcmp + (uint32_t)((q + (v[k].step << LOG_NT)) >> 32);
             asm volatile("prefetch.global.L1 [%0];" ::"l"(nx));
             asm volatile("prefetch.global.L1 [%0];" ::"l"(nx + 16));
         }
@@ -767,16 +814,21 @@ __device__ __forceinline__ void hot_tile(VoiceRegs (&v)[V], const RenderArgs& a,
 #pragma unroll
             for (int k = 0; k < V; ++k) {
                 v[k].level = __fmaf_rn(v[k].level, e[k].em, e[k].ea);
-                const float2 t = __ldg(a.pcmp + (uint32_t)(q[k] >> 32));
-                const float fl = __uint2float_rn((uint32_t)q[k]);
+                const float2* pt;
+                asm("mad.wide.u32 %0, %1, 8, %2;" : "=l"(pt) : "r"(qh[k]), "l"(a.pcmp));
+                const float2 t = __ldg(pt);
+                const float fl = __uint2float_rn(ql[k]);
                 const float s = STRICT ? __fadd_rn(t.x, __fmul_rn(t.y, fl)) : __fmaf_rn(t.y, fl, t.x);
                 y[k] = biquad_fm<STRICT, FM>(v[k], __fmul_rn(s, v[k].level));
-                q[k] += v[k].step;
+                asm("add.cc.u32 %0, %0, %2;\n\taddc.u32 %1, %1, %3;"
+                    : "+r"(ql[k]), "+r"(qh[k])
+                    : "r"((uint32_t)v[k].step), "r"((uint32_t)(v[k].step >> 32)));
             }
             emit<FACTOR, STRICT, V>(sm, lane, i, y, v);
         }
 #pragma unroll
-        for (int k = 0; k < V; ++k) v[k].phase = q[k] - ((uint64_t)v[k].base << 32);
+        for (int k = 0; k < V; ++k)
+            v[k].phase = (((uint64_t)qh[k] << 32) | ql[k]) - ((uint64_t)v[k].base << 32);
     } else {
 #pragma unroll
         for (uint32_t i = 0; i < NT; ++i) {
@@ -969,8 +1021,9 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
             const uint32_t h = lane & 1u;
             if constexpr (FACTOR) {
                 // The gains hold for the whole tile (only a gate row changes
-                // them). Slot = sum over lanes of sample x gain, as four
-                // chains of eight products in lane order, then a pair tree.
+                // them). Slot = sum over lanes of sample x gain: per half-warp
+                // two packed chains of four (even lanes, odd lanes) in lane
+                // order, each pair then added, then the halves.
                 sm[SMG_OFF + lane] = v[0].gl;
                 sm[SMG_OFF + SMG_ROW + lane] = v[0].gr;
                 __syncwarp();
@@ -980,16 +1033,15 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                     float s[2];
 #pragma unroll
                     for (int c = 0; c < 2; ++c) {
-                        float t = 0.0f;
+                        float2 t = make_float2(0.0f, 0.0f);
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const float4 yq = y4[4 * c + q], gq = g4[4 * c + q];
-                            t = q ? __fmaf_rn(yq.x, gq.x, t) : __fmul_rn(yq.x, gq.x);
-                            t = __fmaf_rn(yq.y, gq.y, t);
-                            t = __fmaf_rn(yq.z, gq.z, t);
-                            t = __fmaf_rn(yq.w, gq.w, t);
+                            t = q ? fma2_rn(make_float2(yq.x, yq.y), make_float2(gq.x, gq.y), t)
+                                  : mul2_rn(make_float2(yq.x, yq.y), make_float2(gq.x, gq.y));
+                            t = fma2_rn(make_float2(yq.z, yq.w), make_float2(gq.z, gq.w), t);
                         }
-                        s[c] = t;
+                        s[c] = __fadd_rn(t.x, t.y);
                     }
                     __syncwarp();
                     const float sum = __fadd_rn(s[0], s[1]);
@@ -1001,21 +1053,18 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                     float s[2], u[2];
 #pragma unroll
                     for (int c = 0; c < 2; ++c) {
-                        float t = 0.0f, w = 0.0f;
+                        float2 t = make_float2(0.0f, 0.0f), w = t;
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const float4 gq = g4[4 * c + q], yq = y4[4 * c + q], zq = z4[4 * c + q];
-                            t = q ? __fmaf_rn(yq.x, gq.x, t) : __fmul_rn(yq.x, gq.x);
-                            w = q ? __fmaf_rn(zq.x, gq.x, w) : __fmul_rn(zq.x, gq.x);
-                            t = __fmaf_rn(yq.y, gq.y, t);
-                            w = __fmaf_rn(zq.y, gq.y, w);
-                            t = __fmaf_rn(yq.z, gq.z, t);
-                            w = __fmaf_rn(zq.z, gq.z, w);
-                            t = __fmaf_rn(yq.w, gq.w, t);
-                            w = __fmaf_rn(zq.w, gq.w, w);
+                            const float2 g0 = make_float2(gq.x, gq.y), g1 = make_float2(gq.z, gq.w);
+                            t = q ? fma2_rn(make_float2(yq.x, yq.y), g0, t) : mul2_rn(make_float2(yq.x, yq.y), g0);
+                            w = q ? fma2_rn(make_float2(zq.x, zq.y), g0, w) : mul2_rn(make_float2(zq.x, zq.y), g0);
+                            t = fma2_rn(make_float2(yq.z, yq.w), g1, t);
+                            w = fma2_rn(make_float2(zq.z, zq.w), g1, w);
                         }
-                        s[c] = t;
-                        u[c] = w;
+                        s[c] = __fadd_rn(t.x, t.y);
+                        u[c] = __fadd_rn(w.x, w.y);
                     }
                     __syncwarp();
                     const float sum = __fadd_rn(s[0], s[1]), sum2 = __fadd_rn(u[0], u[1]);
