@@ -305,7 +305,10 @@ __global__ void __launch_bounds__(256) kb_sort_count(const BatchHeader* hdr, con
     for_items<K_SORT>(hdr, plan, [&](uint32_t j, uint32_t c, uint32_t m) {
         const JobDesc& d = jobs[j];
         if (p >= d.sort_passes) return;
-        sort_count_body<RB>(d.pa, d.sort, p ? d.keys[p & 1u] : nullptr, RB * p, d.counts, c, m);
+        // Pass 0 keeps the keys it computes in idx[0] (free until pass 1
+        // writes it) for its scatter.
+        sort_count_body<RB>(d.pa, d.sort, p ? d.keys[p & 1u] : nullptr, RB * p, d.counts, c, m, nullptr,
+                            p ? nullptr : d.idx[0]);
     });
 }
 
@@ -327,7 +330,7 @@ __global__ void __launch_bounds__(256) kb_sort_scatter(const BatchHeader* hdr, c
         const JobDesc& d = jobs[j];
         if (p >= d.sort_passes) return;
         const uint32_t cur = p & 1u;
-        sort_scatter_body<RB>(d.pa, d.sort, p ? d.keys[cur] : nullptr, p ? d.idx[cur] : nullptr, d.keys[cur ^ 1u],
+        sort_scatter_body<RB>(d.pa, d.sort, p ? d.keys[cur] : d.idx[0], p ? d.idx[cur] : nullptr, d.keys[cur ^ 1u],
                               d.idx[cur ^ 1u], RB * p, d.counts, c, m);
     });
 }
@@ -701,7 +704,7 @@ int kc_batch_render(kc_batch* b, kc_synth* const* jobs, uint32_t n_jobs, float* 
         ra.env_floor = c.env_floor;
         ra.exp_decay = c.decay_curve == KC_CURVE_EXPONENTIAL;
         ra.exp_release = c.release_curve == KC_CURVE_EXPONENTIAL;
-        d.sort = s->sort;
+        d.sort = block_sort_layout(s, s->bend ? s->chan : nullptr);
         d.ctl = s->ctl;
         d.sel_hist = s->sel_hist;
         d.counts = s->counts;

@@ -340,16 +340,55 @@ __device__ __forceinline__ void commit_body(DevState* st, const uint32_t* total)
 // the region one past the last, so they sort to the end and the gather stops
 // before them: compaction and reordering are one copy of the pool.
 
+// The phase field is the one the voice is predicted to reach halfway through
+// the next block, phase + rate * half, where rate is the base step times the
+// channel's bend at the last gate tile of this block (when bend rows are on),
+// wrapped into the loop of a looping voice and clamped to the field for the
+// rest. Voices at one rate keep the reference's order (shifted by the same
+// amount); voices at different rates -- bends, detunes, transposed notes --
+// drift apart in both directions from the middle of the block instead of all
+// from its start, which halves the average spread of a warp's taps. The sort
+// only orders the pool for the render's locality: the live set and every
+// voice's state are the same under any key.
 struct SortLayout {
     uint32_t bits, region_shift, stage_shift, phase_shift, phase_mask, dead_region;
+    uint32_t half;               // frames to the middle of the next block (0: the current phase)
+    const uint32_t* chan;        // this block's channel rows while bend rows are on, else null
+    uint32_t last_tile;          // the row of `chan` the prediction reads
 };
+
+__device__ __forceinline__ uint32_t predicted_phase(const uint32_t* pool, uint32_t cap, uint32_t i,
+                                                    const SortLayout& L) {
+    const uint32_t ph = pool[F_PHASE_HI * cap + i];
+    if (L.half == 0) return ph;
+    const uint64_t step = ((uint64_t)pool[F_STEP_HI * cap + i] << 32) | pool[F_STEP_LO * cap + i];
+    // Frames in 16.16, at most 2^20 (past any sample), so the bend product
+    // below stays inside 64 bits.
+    uint64_t adv = (step >> 16) * L.half;
+    if (adv > (1ull << 36)) adv = 1ull << 36;
+    if (L.chan) {
+        const uint32_t ch = (pool[F_GATE_SLOT * cap + i] >> 7) & 15u;
+        const uint32_t bend = L.chan[(L.last_tile * KC_BEND_CHANNELS + ch) * KC_CHAN_FIELDS];  // 8.24
+        adv = (adv >> 8) * bend >> 16;  // still 16.16 (the shifts keep the product in 64 bits)
+    }
+    uint64_t p = (uint64_t)ph + (adv >> 16);
+    const uint32_t ls = pool[F_LOOP_START * cap + i], le = pool[F_LOOP_END * cap + i];
+    if ((pool[F_FLAGS * cap + i] & KC_VF_LOOP) && le > ls + 1u && p >= le) {
+        // Half a block rarely crosses more than one loop: one subtraction,
+        // the remainder (a long division) only when it does.
+        p -= le - ls;
+        if (p >= le) p = ls + (p - ls) % (le - ls);
+    }
+    const uint64_t top = (uint64_t)L.phase_mask << L.phase_shift | ((1ull << L.phase_shift) - 1u);
+    return (uint32_t)(p < top ? p : top);
+}
 
 __device__ __forceinline__ uint32_t sort_key(const uint32_t* pool, uint32_t cap, uint32_t i,
                                              const SortLayout& L) {
     const uint32_t stage = pool[F_ENV_STAGE * cap + i];
     uint32_t region = L.dead_region;
     if (stage != ENV_DEAD) region = min(pool[F_REGION * cap + i], L.dead_region - 1u);
-    const uint32_t ph = (pool[F_PHASE_HI * cap + i] >> L.phase_shift) & L.phase_mask;
+    const uint32_t ph = (predicted_phase(pool, cap, i, L) >> L.phase_shift) & L.phase_mask;
     return (region << L.region_shift) | (min(stage, 7u) << L.stage_shift) | ph;
 }
 
@@ -363,13 +402,14 @@ __device__ __forceinline__ uint32_t sort_chunk(uint32_t n, uint32_t nblocks) {
 constexpr uint32_t SORT_RADIX_MIN = 4, SORT_RADIX_MAX = 10, SORT_RADIX_DEFAULT = 8;
 
 // Pass `shift`: count digit occurrences per CTA chunk into counts[d * G + cta].
-// Pass 0 computes keys from the pool; later passes read the key array.
+// Pass 0 computes keys from the pool (and stores them in `keys_save`, when
+// given, for that pass's scatter); later passes read the key array.
 // `totals` (when given) also receives each digit's count over all CTAs, for
 // sort_offsets_body; it must be zero when the pass starts.
 template <uint32_t RB>
 __device__ __forceinline__ void sort_count_body(PoolArgs a, SortLayout L, const uint32_t* keys, uint32_t shift,
                                                 uint32_t* counts, uint32_t cta, uint32_t ctas,
-                                                uint32_t* totals = nullptr) {
+                                                uint32_t* totals = nullptr, uint32_t* keys_save = nullptr) {
     constexpr uint32_t BINS = 1u << RB;
     __shared__ uint32_t h[BINS];
     const uint32_t n = a.st->live_render;
@@ -378,7 +418,13 @@ __device__ __forceinline__ void sort_count_body(PoolArgs a, SortLayout L, const 
     const uint32_t chunk = sort_chunk(n, ctas);
     const uint32_t lo = cta * chunk, hi = min(n, lo + chunk);
     for (uint32_t i = lo + threadIdx.x; i < hi; i += 256u) {
-        const uint32_t k = keys ? keys[i] : sort_key(a.pool, a.cap, i, L);
+        uint32_t k;
+        if (keys) {
+            k = keys[i];
+        } else {
+            k = sort_key(a.pool, a.cap, i, L);
+            if (keys_save) keys_save[i] = k;
+        }
         atomicAdd(&h[(k >> shift) & (BINS - 1u)], 1u);
     }
     __syncthreads();

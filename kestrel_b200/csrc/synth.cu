@@ -56,8 +56,9 @@ __global__ void k_commit(DevState* st, const uint32_t* total) { commit_body(st, 
 
 template <uint32_t RB>
 __global__ void __launch_bounds__(256) k_sort_count(PoolArgs a, SortLayout L, const uint32_t* keys,
-                                                    uint32_t shift, uint32_t* counts, uint32_t* totals) {
-    sort_count_body<RB>(a, L, keys, shift, counts, blockIdx.x, gridDim.x, totals);
+                                                    uint32_t shift, uint32_t* counts, uint32_t* totals,
+                                                    uint32_t* keys_save) {
+    sort_count_body<RB>(a, L, keys, shift, counts, blockIdx.x, gridDim.x, totals, keys_save);
 }
 
 // One warp per digit: 8 digits per CTA.
@@ -80,28 +81,29 @@ __global__ void __launch_bounds__(256) k_sort_scatter(PoolArgs a, SortLayout L, 
 
 // One LSD pass of the pool sort at digit width RB: count (with the digit
 // totals), the digit-major offsets, scatter. `totals` is zero on entry and on
-// return.
+// return. Pass 0 (kin null) computes the keys once, in the count, into
+// `ksave`, and its scatter reads them from there.
 template <uint32_t RB>
 void sort_pass(cudaStream_t q, uint32_t G, const PoolArgs& pa, const SortLayout& L, const uint32_t* kin,
                const uint32_t* iin, uint32_t* kout, uint32_t* iout, uint32_t shift, uint32_t* counts,
-               uint32_t* totals, uint32_t* total) {
+               uint32_t* totals, uint32_t* total, uint32_t* ksave) {
     constexpr uint32_t BINS = 1u << RB;
-    k_sort_count<RB><<<G, 256, 0, q>>>(pa, L, kin, shift, counts, totals);
+    k_sort_count<RB><<<G, 256, 0, q>>>(pa, L, kin, shift, counts, totals, kin ? nullptr : ksave);
     k_sort_offsets<<<(BINS + 7u) / 8u, 256, 0, q>>>(counts, G, BINS, totals, total);
-    k_sort_scatter<RB><<<G, 256, 0, q>>>(pa, L, kin, iin, kout, iout, shift, counts, totals);
+    k_sort_scatter<RB><<<G, 256, 0, q>>>(pa, L, kin ? kin : ksave, iin, kout, iout, shift, counts, totals);
 }
 
 void sort_pass_rb(uint32_t rb, cudaStream_t q, uint32_t G, const PoolArgs& pa, const SortLayout& L,
                   const uint32_t* kin, const uint32_t* iin, uint32_t* kout, uint32_t* iout, uint32_t shift,
-                  uint32_t* counts, uint32_t* totals, uint32_t* total) {
+                  uint32_t* counts, uint32_t* totals, uint32_t* total, uint32_t* ksave) {
     switch (rb) {
-        case 4: sort_pass<4>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
-        case 5: sort_pass<5>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
-        case 6: sort_pass<6>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
-        case 7: sort_pass<7>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
-        case 9: sort_pass<9>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
-        case 10: sort_pass<10>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
-        default: sort_pass<8>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total); break;
+        case 4: sort_pass<4>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
+        case 5: sort_pass<5>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
+        case 6: sort_pass<6>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
+        case 7: sort_pass<7>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
+        case 9: sort_pass<9>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
+        case 10: sort_pass<10>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
+        default: sort_pass<8>(q, G, pa, L, kin, iin, kout, iout, shift, counts, totals, total, ksave); break;
     }
 }
 
@@ -161,8 +163,9 @@ uint32_t clz32(uint32_t v) { return v ? (uint32_t)__builtin_clz(v) : 32u; }
 uint32_t radix_of(const kc_config& c) { return c.sort_radix_bits ? c.sort_radix_bits : SORT_RADIX_DEFAULT; }
 
 // SortKeyLayout::plan, src/gpu/mod.rs:77-105.
-SortLayout plan_sort(uint32_t n_regions, uint32_t max_len) {
+SortLayout plan_sort(uint32_t n_regions, uint32_t max_len, uint32_t block_frames) {
     SortLayout L{};
+    L.half = block_frames / 2;
     L.dead_region = std::max<uint32_t>(n_regions, 1);
     const uint32_t region_bits = 32 - clz32(L.dead_region);
     const uint32_t stage_bits = 3;
@@ -395,13 +398,15 @@ int enqueue_block(kc_synth* s, const uint32_t* d_gates, const uint32_t* d_chan, 
     } else {
         const uint32_t passes = (s->sort.bits + s->radix - 1) / s->radix;
         const uint32_t G = s->compact_ctas;
+        const SortLayout L = block_sort_layout(s, bend ? d_chan : nullptr);
         int cur = 0;
         for (uint32_t p = 0; p < passes; ++p) {
             const uint32_t shift = s->radix * p;
             const uint32_t* kin = p == 0 ? nullptr : s->keys[cur];
             const uint32_t* iin = p == 0 ? nullptr : s->idx[cur];
-            sort_pass_rb(s->radix, q, G, pa, s->sort, kin, iin, s->keys[cur ^ 1], s->idx[cur ^ 1], shift, s->counts,
-                         s->sort_totals, s->total + 1);
+            // Pass 0 writes keys[1] and idx[1]: idx[0] holds its computed keys.
+            sort_pass_rb(s->radix, q, G, pa, L, kin, iin, s->keys[cur ^ 1], s->idx[cur ^ 1], shift, s->counts,
+                         s->sort_totals, s->total + 1, s->idx[0]);
             cur ^= 1;
         }
         k_sort_gather<<<s->pool_ctas, 256, 0, q>>>(pa, s->idx[cur]);
@@ -553,7 +558,7 @@ int kc_synth_create(const kc_config* cfg, const int16_t* pool, uint64_t pool_len
     s->params_per = params_len;
     s->n_slots = cfg->max_param_variants;
     s->pcm_len = pool_len;
-    s->sort = plan_sort(n_regions, max_sample_len);
+    s->sort = plan_sort(n_regions, max_sample_len, cfg->block_frames);
     s->n_regions = n_regions;
     s->max_sample_len = max_sample_len;
 

@@ -112,4 +112,14 @@ namespace kc {
 inline bool sort_this_block(const kc_synth* s) {
     return s->cfg.sort_voices != 0 && s->blocks % s->cfg.sort_voices == 0;
 }
+
+// The pool sort's layout for the block being enqueued: `chan` is its channel
+// rows when bend rows are on (the predicted phase reads the bend of their last
+// tile), else null.
+inline SortLayout block_sort_layout(const kc_synth* s, const uint32_t* chan) {
+    SortLayout L = s->sort;
+    L.chan = chan;
+    L.last_tile = s->tiles - 1u;
+    return L;
+}
 }  // namespace kc
