@@ -16,14 +16,20 @@ configurations describe; no public dataset is involved):
 
 Measurement. A driver (the C++ restatement of src/driver.rs) renders a
 pre-roll until the pool reaches its steady state. Then:
-  e2e    W + K blocks through the C ABI with host buffers (kc_set_gates,
-         kc_set_channels, kc_spawn, kc_render): host->device copies of the
-         block's inputs and the device->host read of the stereo block are
-         inside each timed step; the driver's own preparation is not.
-  value  a clone of the context at the same state (kc_synth_clone) replays
-         the same W + K recorded blocks from HBM (kc_enqueue_block_device),
-         K timed back to back with CUDA events on the context's stream.
-The two renders are checked to be byte-identical.
+  serial W + K blocks through the C ABI with host buffers (kc_set_gates,
+         kc_set_channels, kc_spawn, kc_render), one at a time; records the
+         blocks' inputs (reported as measured.e2e_serial).
+  e2e    a clone of the context at the same state replays the recorded host
+         buffers through the pipelined form of the same calls: the next
+         block's inputs are staged (kc_set_* / kc_spawn) while this one
+         renders, between kc_render_begin and kc_render_end. The host->device
+         copies of every block's inputs and the device->host read of its
+         stereo block are inside the timed region; the driver's own
+         preparation is not.
+  value  another clone replays the same W + K recorded blocks from HBM
+         (kc_enqueue_block_device), K timed back to back with CUDA events on
+         the context's stream.
+The three renders are checked to be byte-identical.
 
 Metric: voice-samples/s = sum over blocks of (voices rendered x 4096) / time;
 x-realtime = audio seconds / time.
@@ -225,10 +231,13 @@ def run_cuda(args, world, rank, local):
         drv.finish(A.stats().active_voices)
     t_pre = time.perf_counter() - t_pre
     B = A.clone()
+    C = A.clone()
 
-    # e2e: W + K blocks through the C ABI with host buffers; record inputs.
+    # The serial host-buffer form: W + K blocks through the C ABI as the
+    # reference's loop makes them (kc_set_gates, kc_set_channels, kc_spawn,
+    # kc_render per block); records the blocks' inputs.
     W, K = args.warmup, args.steps
-    rec, e2e_t, e2e_units, h2d, d2h = [], 0.0, 0, 0, 0
+    rec, ser_t, e2e_units, h2d, d2h = [], 0.0, 0, 0, 0
     outs_a = []
     for i in range(W + K):
         live = A.stats().active_voices
@@ -242,10 +251,35 @@ def run_cuda(args, world, rank, local):
         rec.append((blk, n_render))
         outs_a.append(out.copy())
         if i >= W:
-            e2e_t += t1 - t0
+            ser_t += t1 - t0
             e2e_units += n_render * bf
             h2d += blk.gates.nbytes + blk.chan.nbytes + blk.cmds.nbytes
             d2h += out.nbytes + 64
+
+    # e2e: the same blocks' host buffers through the pipelined form of the
+    # same calls on a second clone -- kc_render_begin returns once the block
+    # is enqueued, and the next block's kc_set_* / kc_spawn stage its inputs
+    # while this one renders (they wait only for its input copies), then
+    # kc_render_end reads the block back. Every step's host-to-device copies
+    # and its read-back are inside the timed region; the driver's
+    # preparation is not (as in the serial form).
+    outs_c = []
+    for i in range(W):
+        H.feed(C, rec[i][0])
+        C.render(out)
+        outs_c.append(out.copy())
+    t0 = time.perf_counter()
+    if K:
+        H.feed(C, rec[W][0])
+        C.render_begin()
+        for i in range(W + 1, W + K):
+            H.feed(C, rec[i][0])
+            C.render_end(out)
+            outs_c.append(out.copy())
+            C.render_begin()
+        C.render_end(out)
+        outs_c.append(out.copy())
+    e2e_t = time.perf_counter() - t0
 
     # value: replay the recorded blocks from HBM on the clone.
     dev = []
@@ -290,10 +324,12 @@ def run_cuda(args, world, rank, local):
     units = sum(n for _, n, *_ in dev[W:]) * bf
     # determinism: the replay must equal the host-buffer render byte for byte
     same = all(np.array_equal(e[5].cpu().numpy(), outs_a[i]) for i, e in enumerate(dev))
+    same = same and all(np.array_equal(o, outs_a[i]) for i, o in enumerate(outs_c))
     launches = B.launches_total() - launches0  # kernel launches of the K timed blocks
 
     res = {
-        "units": units, "ms": dt_ms, "e2e_units": e2e_units, "e2e_s": e2e_t, "h2d": h2d // max(K, 1),
+        "units": units, "ms": dt_ms, "e2e_units": e2e_units, "e2e_s": e2e_t, "serial_s": ser_t,
+        "h2d": h2d // max(K, 1),
         "d2h": d2h // max(K, 1), "render_ms": passes["render"] / max(nblocks, 1), "passes": passes,
         "nblocks": nblocks, "mean_live": float(np.mean([n for _, n, *_ in dev[W:]])),
         "same": same, "clocks": clk, "launches": launches, "preroll_s": t_pre, "preroll": preroll,
@@ -301,6 +337,7 @@ def run_cuda(args, world, rank, local):
         "steal_percent": cfg.max_steal_percent, "stolen": B.stats().stolen, "dropped": B.stats().dropped,
         "hot_share": ut / at if at else None,
     }
+    C.close()
     B.close()
     A.close()
     return res
@@ -640,7 +677,10 @@ def main(argv=None):
             "config": bench_config(args, world),
             "measured": {"mean_voices_rendered": round(n_render_mean), "preroll_blocks": r["preroll"],
                          "replay_equals_host_render": r["same"], "stolen": r["stolen"],
-                         "hot_path_share": r["hot_share"]},
+                         "hot_path_share": r["hot_share"],
+                         # the host-buffer blocks one at a time (kc_render per
+                         # block, no staging ahead), rank 0
+                         "e2e_serial": r["e2e_units"] / r["serial_s"] if r["serial_s"] > 0 else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "k_render",
                          "algorithmic_bytes_per_launch": bytes_launch,

@@ -108,12 +108,14 @@ struct VoiceRegs {
     float level;
     float gl, gr, bgl, bgr;
     float z1, z2;
-    // region params in force
-    float ar, ae, dc, dt, sus, rc, b0, b1, a1, a2;
+    // region params in force: the filter; the envelope's rates and levels
+    // are read from the params table where they are needed (env_params), so
+    // they hold no registers through the hot tiles
+    float b0, b1, a1, a2;
     bool filt;
     bool loop_en, lur;
     uint32_t params_base, variant, born, born_gate;
-    uint32_t slot, ordinal, start_rel, stop_rel, channel;
+    uint32_t slot, ordinal, start_rel, stop_rel;
     bool neutral;   // dead, and set to contribute exactly +0 on every path (neutralize)
 };
 
@@ -136,21 +138,38 @@ __device__ __forceinline__ void neutralize(VoiceRegs& v, const RenderArgs& a) {
     v.neutral = true;
 }
 
-__device__ __forceinline__ void load_params(VoiceRegs& v, const RenderArgs& a, uint32_t variant) {
-    const uint32_t s = variant < a.n_slots ? variant : 0u;
-    const float4* p = reinterpret_cast<const float4*>(a.params + (size_t)s * a.params_per + v.params_base);
-    const float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2);
-    v.ar = q0.x; v.ae = q0.y; v.dc = q0.z; v.dt = q0.w;
-    v.sus = q1.x; v.rc = q1.y; v.b0 = q1.z; v.b1 = q1.w;
+// The voice's params entry: three float4 words (kc_region_params).
+__device__ __forceinline__ const float4* params_entry(const VoiceRegs& v, const RenderArgs& a) {
+    const uint32_t s = v.variant < a.n_slots ? v.variant : 0u;
+    return reinterpret_cast<const float4*>(a.params + (size_t)s * a.params_per + v.params_base);
+}
+
+__device__ __forceinline__ void load_params(VoiceRegs& v, const RenderArgs& a) {
+    const float4* p = params_entry(v, a);
+    const float4 q1 = __ldg(p + 1), q2 = __ldg(p + 2);
+    v.b0 = q1.z; v.b1 = q1.w;
     v.a1 = q2.x; v.a2 = q2.y;
     v.filt = (__float_as_uint(q2.z) & KC_RP_FILTER) != 0u;
+}
+
+// The envelope's rates and levels of the params entry in force (the table
+// does not change during a block, and the entry only at a gate row's
+// variant switch).
+struct EnvParams {
+    float ar, ae, dc, dt, sus, rc;
+};
+__device__ __forceinline__ EnvParams env_params(const VoiceRegs& v, const RenderArgs& a) {
+    const float4* p = params_entry(v, a);
+    const float4 q0 = __ldg(p);
+    const float2 q1 = __ldg(reinterpret_cast<const float2*>(p + 1));
+    return EnvParams{q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
 }
 
 // Per-frame voice step. Returns the filtered, faded sample y (before the
 // stereo gains). Mirrors src/cpu.rs:490-601 for one frame; the caller has
 // already applied the f < start_rel and DEAD gates.
 template <int INTERP, bool STRICT, bool F32>
-__device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, uint32_t f,
+__device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, const EnvParams& p, uint32_t f,
                                              bool looping) {
     const uint32_t idx = (uint32_t)(v.phase >> 32);
     if (!looping && idx >= v.len) {
@@ -159,24 +178,24 @@ __device__ __forceinline__ float voice_frame(VoiceRegs& v, const RenderArgs& a, 
     }
     // Envelope before the sample (src/cpu.rs:508-549).
     if (v.stage == ENV_ATTACK) {
-        v.level = __fadd_rn(v.level, v.ar);
-        if (v.level >= v.ae) {
+        v.level = __fadd_rn(v.level, p.ar);
+        if (v.level >= p.ae) {
             v.stage = ENV_DECAY;
             v.level = 1.0f;
         }
     } else if (v.stage == ENV_DECAY) {
-        v.level = a.exp_decay ? __fmul_rn(v.level, v.dc) : __fsub_rn(v.level, v.dc);
-        if (v.level <= v.dt) {
-            if (v.sus <= a.env_floor) {
+        v.level = a.exp_decay ? __fmul_rn(v.level, p.dc) : __fsub_rn(v.level, p.dc);
+        if (v.level <= p.dt) {
+            if (p.sus <= a.env_floor) {
                 v.stage = ENV_DEAD;
                 v.level = 0.0f;
             } else {
                 v.stage = ENV_SUSTAIN;
-                v.level = v.sus;
+                v.level = p.sus;
             }
         }
     } else if (v.stage == ENV_RELEASE) {
-        v.level = a.exp_release ? __fmul_rn(v.level, v.rc) : __fsub_rn(v.level, v.rc);
+        v.level = a.exp_release ? __fmul_rn(v.level, p.rc) : __fsub_rn(v.level, p.rc);
         if (v.level <= a.env_floor) {
             v.stage = ENV_DEAD;
             v.level = 0.0f;
@@ -285,14 +304,17 @@ struct EnvStep {
 __device__ __forceinline__ EnvStep env_constants(const VoiceRegs& v, const RenderArgs& a) {
     EnvStep e;
     e.em = 1.0f; e.ea = 0.0f; e.sgn = 1.0f; e.thr = __int_as_float(0x7f800000);  // sustain: never
-    if (v.stage == ENV_ATTACK) {
-        e.ea = v.ar; e.thr = v.ae;
-    } else if (v.stage == ENV_DECAY) {
-        if (a.exp_decay) e.em = v.dc; else e.ea = -v.dc;
-        e.sgn = -1.0f; e.thr = -v.dt;
-    } else if (v.stage == ENV_RELEASE) {
-        if (a.exp_release) e.em = v.rc; else e.ea = -v.rc;
-        e.sgn = -1.0f; e.thr = -a.env_floor;
+    if (v.stage == ENV_ATTACK || v.stage == ENV_DECAY || v.stage == ENV_RELEASE) {
+        const EnvParams p = env_params(v, a);
+        if (v.stage == ENV_ATTACK) {
+            e.ea = p.ar; e.thr = p.ae;
+        } else if (v.stage == ENV_DECAY) {
+            if (a.exp_decay) e.em = p.dc; else e.ea = -p.dc;
+            e.sgn = -1.0f; e.thr = -p.dt;
+        } else {
+            if (a.exp_release) e.em = p.rc; else e.ea = -p.rc;
+            e.sgn = -1.0f; e.thr = -a.env_floor;
+        }
     }
     return e;
 }
@@ -304,12 +326,13 @@ __device__ __forceinline__ bool env_transition(VoiceRegs& v, const RenderArgs& a
         v.stage = ENV_DECAY;
         v.level = 1.0f;
     } else if (v.stage == ENV_DECAY) {
-        if (v.sus <= a.env_floor) {
+        const float sus = env_params(v, a).sus;
+        if (sus <= a.env_floor) {
             v.stage = ENV_DEAD;
             v.level = 0.0f;
         } else {
             v.stage = ENV_SUSTAIN;
-            v.level = v.sus;
+            v.level = sus;
         }
     } else if (v.stage == ENV_RELEASE) {
         v.stage = ENV_DEAD;
@@ -518,10 +541,10 @@ __device__ __forceinline__ void load_voice(VoiceRegs& v, const RenderArgs& a, ui
     v.phase = 0; v.step = 0; v.base_step = 0;
     v.base = 0; v.len = 1; v.ls = 0; v.le = 1;
     v.level = 0.0f; v.gl = v.gr = v.bgl = v.bgr = 0.0f; v.z1 = v.z2 = 0.0f;
-    v.ar = v.ae = v.dc = v.dt = v.sus = v.rc = v.b0 = v.b1 = v.a1 = v.a2 = 0.0f;
+    v.b0 = v.b1 = v.a1 = v.a2 = 0.0f;
     v.filt = false; v.loop_en = false; v.lur = false;
     v.params_base = 0; v.variant = 0; v.born = 0; v.born_gate = 0;
-    v.slot = 0; v.ordinal = 0; v.start_rel = 0; v.stop_rel = 0; v.channel = 0;
+    v.slot = 0; v.ordinal = 0; v.start_rel = 0; v.stop_rel = 0;
     v.neutral = false;
     if (!live) return;
     const uint32_t cap = a.cap;
@@ -558,13 +581,12 @@ __device__ __forceinline__ void load_voice(VoiceRegs& v, const RenderArgs& a, ui
         atomicOr(&a.st->error, ERR_SLOT_RANGE);
         v.slot = 0;
     }
-    v.channel = (v.slot >> 7) & 15u;
     v.born_gate = v.start_rel / a.gate_frames;
     if (v.params_base >= a.params_per) {
         atomicOr(&a.st->error, ERR_PARAMS_RANGE);
         v.params_base = 0;
     }
-    load_params(v, a, v.variant);
+    load_params(v, a);
 }
 
 // Write back what a block changes (src/cpu.rs:605-612).
@@ -591,7 +613,9 @@ __device__ __forceinline__ void tile_update(VoiceRegs& v, const RenderArgs& a, u
         v.level = fminf(v.level, 1.0f);
     }
     if (CHAN && chan_active) {
-        const uint4 row = __ldg(reinterpret_cast<const uint4*>(a.chan) + gt * KC_BEND_CHANNELS + v.channel);
+        // the slot's channel (GateTable::slot, src/voice.rs:260-262: ch * 128 + key)
+        const uint32_t channel = (v.slot >> 7) & 15u;
+        const uint4 row = __ldg(reinterpret_cast<const uint4*>(a.chan) + gt * KC_BEND_CHANNELS + channel);
         if (chan_active & 1u) v.step = scale_step(v.base_step, row.x);
         if (chan_active & 2u) {
             v.gl = __fmul_rn(v.bgl, __uint_as_float(row.y));
@@ -601,7 +625,7 @@ __device__ __forceinline__ void tile_update(VoiceRegs& v, const RenderArgs& a, u
             const bool born_here = v.born != 0u && gt <= v.born_gate;
             if (row.w != v.variant && !born_here) {
                 v.variant = row.w;
-                load_params(v, a, v.variant);
+                load_params(v, a);
             }
         }
     }
@@ -992,15 +1016,19 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
                     put_pair(sm, lane, i, yl, yr);
                 }
             } else if (FACTOR) {
+                const EnvParams ep = env_params(v[0], a);
 #pragma unroll 1
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
                     const uint32_t f = f0 + i;
                     float y = 0.0f;
                     if (v[0].stage != ENV_DEAD && f >= v[0].start_rel)
-                        y = voice_frame<INTERP, STRICT, F32>(v[0], a, f, looping[0]);
+                        y = voice_frame<INTERP, STRICT, F32>(v[0], a, ep, f, looping[0]);
                     sm[i * SMY_ROW + lane] = y;
                 }
             } else {
+                EnvParams ep[V];
+#pragma unroll
+                for (int k = 0; k < V; ++k) ep[k] = env_params(v[k], a);
 #pragma unroll 1
                 for (uint32_t i = 0; i < MIX_TILE; ++i) {
                     const uint32_t f = f0 + i;
@@ -1008,7 +1036,7 @@ __device__ __forceinline__ void render_batches(const RenderArgs& a, float* sm, u
 #pragma unroll
                     for (int k = 0; k < V; ++k) {
                         if (v[k].stage != ENV_DEAD && f >= v[k].start_rel) {
-                            const float y = voice_frame<INTERP, STRICT, F32>(v[k], a, f, looping[k]);
+                            const float y = voice_frame<INTERP, STRICT, F32>(v[k], a, ep[k], f, looping[k]);
                             if (k == 0) acc_out<STRICT, true>(yl, yr, y, v[k]);
                             else acc_out<STRICT, false>(yl, yr, y, v[k]);
                         }

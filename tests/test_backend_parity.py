@@ -88,6 +88,31 @@ def test_parity_spans_broken_by_gate_rows(vpl):
 
 
 @gpu
+@pytest.mark.parametrize("steps", ["ratio", "unit", "integral"])
+def test_parity_loop_wraps_inside_hot_tiles(steps):
+    """Sustained voices in short loops that end at the sample's end (the
+    shape of a real bank's looped zones): most lanes pass their loop end every
+    few tiles, read the seam tap (loop_end - 1, whose neighbour is
+    loop_start) at fractional phases, and switch between the hot paths and
+    the general one around each wrap; spans of 2 to 400 frames cover one wrap
+    a tile and loops short enough to wrap twice in one. Every pool field, the
+    filter state included, must equal the CPU reference's."""
+    sc = make_scenario(seed=21, max_voices=40000, n_blocks=4, spawn_per_block=(9000, 12000), release_rate=0.02,
+                       steps=steps, chan=steps == "ratio", bend_prob=0.5, block_frames=4096)
+    rng = np.random.default_rng(22)
+    for blk in sc.blocks:
+        c = blk.cmds
+        span = rng.integers(17, 401, c.size).astype(np.uint32)
+        short = rng.random(c.size) < 0.05
+        span[short] = rng.integers(2, 17, int(short.sum()))
+        c["loop_end"] = c["smp_len"]
+        c["loop_start"] = c["smp_len"] - np.minimum(span, c["smp_len"] - 1)
+        c["flags"] = np.where(rng.random(c.size) < 0.85, N.VF_LOOP, N.VF_LOOP | N.VF_LOOP_UNTIL_RELEASE)
+        c["phase_hi"] = c["loop_start"] + (rng.random(c.size) * (c["loop_end"] - c["loop_start"])).astype(np.uint32)
+    _compare(sc)
+
+
+@gpu
 @pytest.mark.parametrize("interp", [N.INTERP_LINEAR, N.INTERP_NEAREST])
 def test_parity_integral_steps(interp):
     """Whole-number steps (1, 2, 3) with zero phase fractions: the
